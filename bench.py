@@ -1,0 +1,334 @@
+"""Benchmark: plain Ligerito prove at 2^24 (config_24, coefficients from
+SplitMix64 seed 1) on B200, through liblgpu.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one complete proof (commit, fold, recursive commits, sumcheck
+rounds, openings; Fiat-Shamir on the host) of a polynomial already resident
+in HBM.  Prints one JSON line (rank 0).  N > 1 (torchrun, one process per
+GPU) runs independent replicas: a proof does not shard, so ranks prove
+their own polynomials and only timings are reduced (max over ranks).
+
+--impl reference times the reference's CPU implementation: this
+environment cannot build the Rust crate, so the arm runs the C
+restatement of it under oracle/ (same algorithms, bit-serial field
+multiply, OpenMP where the reference uses rayon) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+METRIC = "prove ms at 2^24 vs host CPU; mixed-size proofs/s + p99, batched vs plain GPU"
+WORKLOAD = "plain single proof at 2^24 (config_24, SplitMix64 seed 1)"
+L2_BYTES = 126 * 2**20
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_per_launch(kernel: str):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    p = ROOT / "profiles" / "dram_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d.get(kernel)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in pathlib.Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def cpu_baseline(log_size: int = 24, seed: int = 1, threads: int | None = None):
+    """The oracle (C restatement of the reference CPU prover) on host cores:
+    one full proof of the same workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import lgref
+
+    threads = threads or os.cpu_count() or 1
+    cfg = lgref.config_make(log_size)
+    poly = lgref.splitmix(seed, 1 << log_size)
+    t0 = time.perf_counter()
+    lgref.prove(cfg, poly, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return dt * 1e3, threads
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import lgref
+
+    threads = os.cpu_count() or 1
+    # warm-up on a small config (loads the library, spins up the thread pool)
+    for _ in range(min(args.warmup, 1)):
+        lgref.prove(lgref.config_make(16), lgref.splitmix(16, 1 << 16), nthreads=threads)
+    steps = max(1, min(args.steps, 3))  # one full 2^24 proof per step, bounded
+    times = [cpu_baseline(24, 1, threads)[0] for _ in range(steps)]
+    ms = sum(times) / len(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
+        "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (GF(2^32))", "data": "synthetic (SplitMix64 seed 1)",
+        "config": {"workload": WORKLOAD, "log_size": 24, "inputs": "host memory"},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full 2^24 proof(s) by the C restatement under oracle/ "
+                                   "(the Rust reference cannot be built here)"},
+        "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = _env_rank()
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as g
+
+    lg = g.load_package()
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("lg_replicas", ROOT / "ligerito-rust_b200" / "replicas.py")
+    rep = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(rep)
+
+    dev = local
+    torch.cuda.set_device(dev)
+    ctx = lg.Context(dev)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=f"cuda:{dev}")
+    cfg = lg.hardcoded_config_24()
+    seed = 1 + rank  # independent replica inputs; rank 0 proves the seed-1 workload
+    poly = lg.splitmix_coeffs_device(seed, cfg.poly_len, ctx)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=f"cuda:{dev}")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        lg.prover(cfg, poly, ctx)
+    torch.cuda.synchronize()
+    barrier()
+
+    # --- device-resident input: per-step CUDA events on the library stream,
+    #     an L2 flush (write of 2x L2) between steps, outside the events
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = ctx.launch_count
+    with ClockSampler(dev) as clk:
+        for e0, e1 in evs:
+            with torch.cuda.stream(stream):
+                flush.fill_(rank + 1)
+                e0.record(stream)
+            proof = lg.prover(cfg, poly, ctx)
+            e1.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launch_count - launches0
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total = rep.reduce_max(sum(step_ms))
+    ms_per_proof = total / (args.steps * world)
+    clocks = clk.summary()
+    proof_bytes = len(proof.to_bytes())
+
+    # --- end to end through the public API: pinned host input, proof
+    #     serialized to host memory, inside the events
+    host = torch.empty(cfg.poly_len, dtype=torch.int32, pin_memory=True)
+    host.copy_(poly.cpu())
+    host_np = host.numpy().view("uint32")
+    barrier()
+    e2e = []
+    for _ in range(max(2, args.steps // 2)):
+        with torch.cuda.stream(stream):
+            flush.fill_(rank + 2)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        pb = lg.prover(cfg, host_np, ctx).to_bytes()
+        b.record(stream)
+        b.synchronize()
+        e2e.append(a.elapsed_time(b))
+    e2e_ms = rep.reduce_max(sum(e2e)) / (len(e2e) * world)
+
+    # --- roofline of the dominant kernel: per-kernel CUDA events on the
+    #     launching stream (a separate pass, not the timed one)
+    ctx.set_kernel_timing(True)
+    ctx.reset_kernel_stats()
+    lg.prover(cfg, poly, ctx)
+    stats = ctx.kernel_stats()
+    ctx.set_kernel_timing(False)
+    top = max(stats.items(), key=lambda kv: kv[1][1])
+    name, (n_launch, tot_ms) = top
+    avg_s = tot_ms / n_launch / 1e3
+    # fft_pass at L=18 on the 64-column first-round matrix: every launch
+    # reads and writes the whole 4 x 2^18 x 64 word matrix once
+    algo_bytes = 2 * 4 * (4 << 18) * 64 if name.startswith("fft_pass_L18") else None
+    peak, peak_kind = _peaks()
+    achieved = (algo_bytes / avg_s / 1e9) if algo_bytes else None
+    mults = (64 * 4 * (1 << 17) * 6) if name.startswith("fft_pass_L18_K6") else None  # GF mults per launch
+    roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1) if achieved else None,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": round(achieved / peak, 4) if achieved else None,
+                "traffic": _traffic_per_launch(name), "avg_launch_ms": round(avg_s * 1e3, 4),
+                "gf_mults_per_launch": mults,
+                "gf_mults_per_s": round(mults / avg_s, 1) if mults else None,
+                "kernel_ms": {k: round(v[1], 4) for k, v in sorted(stats.items(), key=lambda kv: -kv[1][1])}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ms, cores = cpu_baseline(24, 1)
+        cpu = {"value": round(ms, 1), "unit": "ms", "cores": cores, "kind": "port",
+               "sample": "1 full 2^24 proof (config_24, seed 1) by the C restatement under oracle/"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms_per_proof, 4), "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps, 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u32 (GF(2^32))",
+            "data": "synthetic (SplitMix64 coefficients, seed 1 + rank)",
+            "config": {"workload": WORKLOAD, "log_size": 24, "parallelism": f"replicas x{world}",
+                       "l2": "flushed between timed steps (write of 2 x L2)", "proof_bytes": proof_bytes},
+            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 4 * cfg.poly_len,
+                    "d2h_bytes_per_step": len(pb)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def run_micro(args):
+    """Kernel microbenchmarks of the 2^24 workload: the first-round RS encode +
+    Merkle commit (2^18 x 64 -> 2^20 x 64), and batched fft / ifft of
+    256 MiB at 2^16 / 2^20 / 2^22 points (SplitMix64 seed 1)."""
+    import torch
+
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as g
+
+    lg = g.load_package()
+    ctx = lg.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device="cuda:0")
+    w = args.workload
+    if w == "commit24":
+        poly = lg.splitmix_coeffs_device(1, 64 << 18, ctx)
+        run = lambda: lg.ligero_commit(poly, 18, 64, ctx)  # noqa: E731
+        unit_count, metric = 1, "first-round RS encode + Merkle commit at 2^24 (2^18 x 64), ms"
+    else:
+        inv = w.startswith("ifft")
+        log_n = int(w[4:] if inv else w[3:])
+        data = lg.splitmix_coeffs_device(1, 1 << 26, ctx)
+        fn = lg.ifft if inv else lg.fft
+        run = lambda: fn(data, log_n, ctx)  # noqa: E731
+        unit_count, metric = 1, f"{'ifft' if inv else 'fft'} of 256 MiB as {1 << (26 - log_n)} x 2^{log_n} points, ms"
+    for _ in range(args.warmup):
+        run()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        run()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    ctx.set_kernel_timing(True)
+    ctx.reset_kernel_stats()
+    run()
+    stats = ctx.kernel_stats()
+    print(json.dumps({"workload": w, "metric": metric, "value": round(statistics.median(times), 4) if times else None,
+                      "unit": "ms", "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                      "kernel_ms": {k: [v[0], round(v[1], 4)] for k, v in stats.items()}}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="prove24",
+                    choices=["prove24", "commit24", "fft16", "fft20", "fft22", "ifft16", "ifft20", "ifft22"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    elif args.workload != "prove24":
+        run_micro(args)
+    else:
+        args.warmup = max(args.warmup, 3)
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

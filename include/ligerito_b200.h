@@ -1,0 +1,187 @@
+/*
+ * ligerito_b200.h -- C ABI of liblgpu.so, the B200 (sm_100a) implementation
+ * of the Ligerito prover hot path of ashutosh1206/ligerito-rust.
+ *
+ * Plain C types only: host pointers, device pointers (as plain pointers),
+ * sizes.  Every call returns an lg_status and never aborts the process;
+ * where the reference panics, the call returns an error status instead.
+ * The field is GF(2^32) with x^32 + x^15 + x^9 + x^7 + x^4 + x^3 + 1
+ * (src/binary_field.rs:179-181); elements travel as uint32_t.
+ *
+ * Each declaration names the reference interface it replaces
+ * (path:line inside the reference project).
+ */
+#ifndef LIGERITO_B200_H
+#define LIGERITO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LG_ABI_VERSION 1
+#define LG_MAX_STEPS 8
+#define LG_NUM_QUERIES 148 /* s, src/prover.rs:30 and src/verifier.rs:25 */
+#define LG_FS_SEED 1234u   /* src/prover.rs:29 and src/verifier.rs:24 */
+
+typedef enum lg_status {
+    LG_OK = 0,
+    LG_ERR_INVALID_ARGUMENT = 1, /* null pointer, size out of range */
+    LG_ERR_INVALID_CONFIG = 2,   /* config the reference would panic on */
+    LG_ERR_OUT_OF_MEMORY = 3,    /* device allocation or HBM budget */
+    LG_ERR_CUDA = 4,             /* CUDA runtime error (see lg_ctx_last_error) */
+    LG_ERR_VERIFY_PANIC = 5,     /* the reference verifier would have panicked */
+    LG_ERR_PROVER_ASSERT = 6,    /* a prover-side assert of the reference failed */
+    LG_ERR_NO_DEVICE = 7,        /* no CUDA device / library built without one */
+    LG_ERR_MALFORMED_PROOF = 8   /* proof bytes do not parse */
+} lg_status;
+
+/* Mirrors ProverConfig / VerifierConfig (src/data_structures.rs:9-30) without
+ * the precomputed Reed-Solomon tables, which the context caches:
+ *   initial_dims = (2^initial_log_m, 2^initial_log_n), dims[i] =
+ *   (2^log_m[i], 2^log_n[i]), ks[i], initial_k, recursive_steps.
+ * The verifier reads initial_dim = initial_log_m and log_dims = log_m. */
+typedef struct lg_config {
+    uint32_t recursive_steps;
+    uint32_t initial_log_m;
+    uint32_t initial_log_n;
+    uint32_t initial_k;
+    uint32_t log_m[LG_MAX_STEPS];
+    uint32_t log_n[LG_MAX_STEPS];
+    uint32_t ks[LG_MAX_STEPS];
+} lg_config;
+
+typedef struct lg_ctx lg_ctx;     /* one device, one stream, caches; one host thread */
+typedef struct lg_proof lg_proof; /* FinalizedLigeritoProof<BinaryElem32> */
+
+const char *lg_status_string(lg_status s);
+uint32_t lg_abi_version(void);
+
+/* ---------------------------------------------------------------- configs */
+/* hardcoded_config_20 / hardcoded_config_20_verifier, src/config.rs:6-67 */
+lg_status lg_hardcoded_config_20(lg_config *out);
+/* hardcoded_config_24 / hardcoded_config_24_verifier, src/config.rs:69-134 */
+lg_status lg_hardcoded_config_24(lg_config *out);
+/* Sizes config.rs has no function for (2^16..2^30), by the same pattern:
+ * initial (2^(L-6), 2^6) with k = 6, then (2^(d-4), 2^4) steps from
+ * d = L-6 while d-4 >= 10; L = 16..19 get one step (2^(L-10), 2^4).
+ * Reproduces config 20 and 24 exactly. */
+lg_status lg_config_make(uint32_t log_size, lg_config *out);
+/* The consistency the reference asserts while proving (src/prover.rs,
+ * src/sumcheck_polys.rs:97): LG_OK or LG_ERR_INVALID_CONFIG. */
+lg_status lg_config_validate(const lg_config *cfg, uint64_t poly_len);
+
+/* ---------------------------------------------------------------- context */
+/* hbm_budget_bytes = 0: no budget.  Fails with LG_ERR_NO_DEVICE without a GPU. */
+lg_status lg_ctx_create(int device, uint64_t hbm_budget_bytes, lg_ctx **out);
+void lg_ctx_destroy(lg_ctx *ctx);
+const char *lg_ctx_last_error(const lg_ctx *ctx);
+void *lg_ctx_stream(lg_ctx *ctx);        /* the cudaStream_t every call is issued on */
+lg_status lg_ctx_synchronize(lg_ctx *ctx);
+uint64_t lg_ctx_launch_count(const lg_ctx *ctx); /* kernels this context launched */
+/* Per-kernel CUDA-event timing (off by default); stats accumulate until reset. */
+lg_status lg_ctx_set_kernel_timing(lg_ctx *ctx, int enabled);
+lg_status lg_ctx_kernel_stats(lg_ctx *ctx, uint32_t index, char *name, size_t name_cap,
+                              uint64_t *launches, double *total_ms); /* INVALID_ARGUMENT past end */
+lg_status lg_ctx_reset_kernel_stats(lg_ctx *ctx);
+uint64_t lg_ctx_device_bytes_in_use(const lg_ctx *ctx);
+
+/* ------------------------------------------------------------ prove/verify */
+/* prover::<BinaryElem32>(config, poly), src/prover.rs:15.  `poly` holds
+ * `len` coefficients on the host (poly_on_device = 0) or on this context's
+ * device (1); the caller keeps ownership.  The Fiat-Shamir seed is 1234 and
+ * s = 148 as in the reference.  *out is freed with lg_proof_free. */
+lg_status lg_prove(lg_ctx *ctx, const lg_config *cfg, const uint32_t *poly, uint64_t len,
+                   int poly_on_device, lg_proof **out);
+
+/* verifier::<BinaryElem32>(config, proof), src/verifier.rs:10.  LG_OK with
+ * *accepted = the reference's return value; LG_ERR_VERIFY_PANIC (accepted =
+ * 0) where the reference panics (Merkle / Ligero asserts, malformed sizes). */
+lg_status lg_verify(lg_ctx *ctx, const lg_config *cfg, const lg_proof *proof, int *accepted);
+
+/* Canonical byte encoding in the field order of FinalizedLigeritoProof
+ * (src/data_structures.rs:91-103); the reference keeps proofs in memory
+ * only.  buf = NULL queries the size into *len. */
+lg_status lg_proof_serialize(const lg_proof *proof, uint8_t *buf, uint64_t *len);
+lg_status lg_proof_deserialize(const uint8_t *buf, uint64_t len, lg_proof **out);
+void lg_proof_free(lg_proof *proof);
+/* ProofSize::proof_size, src/data_structures.rs:165-194 */
+lg_status lg_proof_size(const lg_proof *proof, uint64_t *bytes);
+
+/* ----------------------------------------------------- kernel entry points
+ * Device pointers belong to the context's device; work is issued on the
+ * context stream and these calls return after it completes. */
+
+/* compute_twiddles(log_n, None), src/binary_fft.rs:30-58; host output of
+ * 2^log_n - 1 heap-ordered entries (log_n in 1..30). */
+lg_status lg_compute_twiddles(uint32_t log_n, uint32_t *out);
+
+/* fft(v, &compute_twiddles(log_n), _), src/binary_fft.rs:4-17, applied in
+ * place to `batch` contiguous vectors of 2^log_n elements. */
+lg_status lg_fft(lg_ctx *ctx, uint32_t *d_data, uint32_t log_n, uint64_t batch);
+/* ifft(v, &compute_twiddles(log_n)), src/binary_fft.rs:19-28, same layout. */
+lg_status lg_ifft(lg_ctx *ctx, uint32_t *d_data, uint32_t log_n, uint64_t batch);
+
+/* ReedSolomonEncoding::new(2^log_m, 2^(log_m+2)).encode_non_systematic on
+ * every column of poly2flatmat: src/reed_solomon.rs:104-113 with
+ * src/ligero.rs:11-38.  d_poly: n columns of 2^log_m (column j at
+ * j*2^log_m); d_encoded: n columns of 2^(log_m+2), column-major. */
+lg_status lg_rs_encode_cols(lg_ctx *ctx, const uint32_t *d_poly, uint32_t log_m, uint32_t n,
+                            uint32_t *d_encoded);
+
+/* ligero_commit, src/ligero.rs:70-95: the encoded matrix (as above) and the
+ * BLAKE3 Merkle tree over its rows (src/merkle_tree.rs:22-60, leaves = rows
+ * as little-endian bytes, src/ligero.rs:53-68).  d_tree receives all layers
+ * leaves first, 32*(2*rows-1) bytes; root (host, 32 bytes) may be NULL. */
+lg_status lg_ligero_commit(lg_ctx *ctx, const uint32_t *d_poly, uint32_t log_m, uint32_t n,
+                           uint32_t *d_encoded, uint8_t *d_tree, uint8_t *root);
+
+/* MultiLinearPoly::partial_eval(rs), src/multilinear_poly.rs:66-87: folds
+ * the top k variables of d_evals (2^log_len) into d_out (2^(log_len-k)). */
+lg_status lg_partial_eval(lg_ctx *ctx, const uint32_t *d_evals, uint32_t log_len,
+                          const uint32_t *rs, uint32_t k, uint32_t *d_out);
+
+/* eval_013_product(f, g), src/multilinear_poly.rs:90-131 -> out[3] (host). */
+lg_status lg_eval_013_product(lg_ctx *ctx, const uint32_t *d_f, const uint32_t *d_g,
+                              uint32_t log_len, uint32_t out[3]);
+
+/* induce_sumcheck_poly_parallel, src/sumcheck_polys.rs:74-160: rows are
+ * host row-major (nrows x 2^nch), queries sorted; basis into d_basis_out
+ * (2^n) and the enforced sum into *enforced_sum. */
+lg_status lg_induce_sumcheck_poly(lg_ctx *ctx, uint32_t n, const uint32_t *rows, uint32_t nrows,
+                                  const uint32_t *v_challenges, uint32_t nch,
+                                  const uint64_t *queries, uint32_t alpha, uint32_t *d_basis_out,
+                                  uint32_t *enforced_sum);
+
+/* ------------------------------------------------ host-side protocol parts
+ * Fiat-Shamir transcript, FS (src/emulated_fs.rs:6-76): running SHA-256
+ * over the seed's LE bytes, absorbed bytes and each squeeze's LE counter. */
+typedef struct lg_transcript lg_transcript;
+lg_status lg_transcript_new(uint32_t seed, lg_transcript **out);        /* FS::new, :12 */
+void lg_transcript_free(lg_transcript *t);
+lg_status lg_transcript_absorb(lg_transcript *t, const uint8_t *bytes, uint64_t len); /* :18 */
+lg_status lg_transcript_squeeze(lg_transcript *t, uint64_t out[2]);     /* :22, u128 low/high */
+lg_status lg_transcript_get_field(lg_transcript *t, uint32_t *out);     /* :34, BinaryElem32 */
+lg_status lg_transcript_get_query(lg_transcript *t, uint64_t n, uint64_t *out); /* :56 */
+/* :61; LG_ERR_INVALID_ARGUMENT where the reference loops forever (n < s) */
+lg_status lg_transcript_get_distinct_queries(lg_transcript *t, uint64_t n, uint64_t s, uint64_t *out);
+
+/* merkle_tree::verify (src/merkle_tree.rs:164-188) with BLAKE3 leaves and
+ * nodes: leaf i = leaves[leaf_off[i] .. leaf_off[i+1]], proof = n_sib
+ * 32-byte siblings.  LG_OK with *ok = the reference's bool, or
+ * LG_ERR_VERIFY_PANIC where it indexes past the proof. */
+lg_status lg_merkle_verify(const uint8_t *root, const uint8_t *proof, uint64_t n_sib, uint64_t depth,
+                           const uint8_t *leaves, const uint64_t *leaf_off, const uint64_t *queries,
+                           uint64_t nq, int *ok);
+
+/* Seeded coefficient generator (SplitMix64; coefficient i = low 32 bits of
+ * output i).  The reference draws unseeded rand::random (src/main.rs:25). */
+lg_status lg_fill_splitmix(lg_ctx *ctx, uint64_t seed, uint32_t *d_out, uint64_t n);
+void lg_fill_splitmix_host(uint64_t seed, uint32_t *out, uint64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIGERITO_B200_H */

@@ -1,0 +1,917 @@
+// C ABI of liblgpu: context, device memory, the prover and verifier
+// protocols (src/prover.rs, src/verifier.rs) driving the kernels of
+// lg_kernels.cu, and the kernel-level entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ligerito_b200.h"
+#include "lg_host.h"
+#include "lg_kernels.h"
+
+using lg::NodeRef;
+
+struct lg_proof {
+    lg::Proof p;
+};
+
+namespace {
+
+struct Code {  // ReedSolomonEncoding::new(m, 4m) tables, src/reed_solomon.rs:49-64
+    uint32_t *tw = nullptr;   // compute_twiddles(log m + 2): 4m - 1 words
+    uint32_t *pis = nullptr;  // compute_pis(m, eval_sk_at_vks(m)): m words
+};
+
+}  // namespace
+
+struct lg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    lgk::Launcher L;
+    uint64_t budget = 0, in_use = 0;
+    std::string err;
+    std::map<uint32_t, Code> codes;       // by log_m
+    std::map<uint32_t, uint32_t *> ffttw;  // by log_n, plain fft twiddles
+    uint8_t *pinned = nullptr;
+    size_t pinned_cap = 0;
+};
+
+namespace {
+
+struct CudaFail {
+    cudaError_t e;
+};
+
+void fail_if(lg_ctx *c, cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        c->err = std::string(what) + ": " + cudaGetErrorString(e);
+        throw CudaFail{e};
+    }
+}
+#define CK(c, expr) fail_if((c), (expr), #expr)
+
+struct OutOfBudget {};
+struct ProverAssert {};
+struct VerifyPanic {};
+struct BadConfig {};
+
+// Stream-ordered device allocation from the device's pool, counted against
+// the context's HBM budget.
+struct DBuf {
+    lg_ctx *c = nullptr;
+    void *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(lg_ctx *ctx, size_t bytes) : c(ctx), n(bytes) {
+        if (c->budget && c->in_use + bytes > c->budget) {
+            c->err = "HBM budget exceeded";
+            throw OutOfBudget{};
+        }
+        cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), c->stream);
+        if (e != cudaSuccess) {
+            c->err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
+            throw OutOfBudget{};
+        }
+        c->in_use += bytes;
+    }
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    DBuf(DBuf &&o) noexcept : c(o.c), p(o.p), n(o.n) { o.p = nullptr; }
+    DBuf &operator=(DBuf &&o) noexcept {
+        if (this != &o) { reset(); c = o.c; p = o.p; n = o.n; o.p = nullptr; }
+        return *this;
+    }
+    void reset() {
+        if (p) { cudaFreeAsync(p, c->stream); c->in_use -= n; p = nullptr; }
+    }
+    ~DBuf() { reset(); }
+    uint32_t *u32() const { return static_cast<uint32_t *>(p); }
+    uint64_t *u64() const { return static_cast<uint64_t *>(p); }
+};
+
+uint8_t *pinned(lg_ctx *c, size_t bytes) {
+    if (bytes > c->pinned_cap) {
+        if (c->pinned) cudaFreeHost(c->pinned);
+        c->pinned = nullptr;
+        size_t cap = std::max<size_t>(bytes, 1 << 20);
+        CK(c, cudaMallocHost((void **)&c->pinned, cap));
+        c->pinned_cap = cap;
+    }
+    return c->pinned;
+}
+
+void sync(lg_ctx *c) { CK(c, cudaStreamSynchronize(c->stream)); }
+
+void h2d(lg_ctx *c, void *dst, const void *src, size_t bytes) {
+    uint8_t *p = pinned(c, bytes);
+    std::memcpy(p, src, bytes);
+    CK(c, cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, c->stream));
+    sync(c);  // the staging buffer is reused by the next transfer
+}
+void d2h(lg_ctx *c, void *dst, const void *src, size_t bytes) {
+    uint8_t *p = pinned(c, bytes);
+    CK(c, cudaMemcpyAsync(p, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    sync(c);
+    std::memcpy(dst, p, bytes);
+}
+
+const Code &get_code(lg_ctx *c, uint32_t log_m) {
+    auto it = c->codes.find(log_m);
+    if (it != c->codes.end()) return it->second;
+    const uint64_t m = 1ull << log_m;
+    std::vector<uint32_t> tw((4 * m) - 1), pis(m);
+    lg::compute_twiddles(log_m + 2, tw.data());
+    lg::compute_pis(m, lg::eval_sk_at_vks(m), pis.data());
+    Code code;
+    CK(c, cudaMalloc(&code.tw, tw.size() * 4));
+    CK(c, cudaMalloc(&code.pis, pis.size() * 4));
+    CK(c, cudaMemcpy(code.tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
+    CK(c, cudaMemcpy(code.pis, pis.data(), pis.size() * 4, cudaMemcpyHostToDevice));
+    return c->codes[log_m] = code;
+}
+
+const uint32_t *get_fft_tw(lg_ctx *c, uint32_t log_n) {
+    auto it = c->ffttw.find(log_n);
+    if (it != c->ffttw.end()) return it->second;
+    std::vector<uint32_t> tw((1ull << log_n) - 1);
+    lg::compute_twiddles(log_n, tw.data());
+    uint32_t *d = nullptr;
+    CK(c, cudaMalloc(&d, tw.size() * 4));
+    CK(c, cudaMemcpy(d, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
+    return c->ffttw[log_n] = d;
+}
+
+// ------------------------------------------------------------ commitment
+struct Witness {  // RecursiveLigeroWitness, src/data_structures.rs:32-40
+    DBuf E;       // column-major encoded matrix, cols x rows
+    DBuf tree;    // all layers, leaves first, 8 words per node
+    uint64_t rows = 0;
+    uint32_t cols = 0;
+    uint8_t root[32];
+};
+
+// ligero_commit (src/ligero.rs:70-95) into caller buffers
+void commit_into(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *E, uint32_t *tree) {
+    const Code &code = get_code(c, log_m);
+    const uint64_t m = 1ull << log_m, rows = 4 * m;
+    CK(c, lgk::rs_scale_spread(c->L, d_poly, code.pis, E, log_m, n));
+    CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, rows, 4, m, 4, false));
+    CK(c, lgk::leaf_hashes(c->L, E, rows, n, tree));
+    CK(c, lgk::merkle_upper(c->L, tree, rows));
+}
+
+Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
+    Witness w;
+    w.rows = 4ull << log_m;
+    w.cols = n;
+    w.E = DBuf(c, w.rows * n * 4);
+    w.tree = DBuf(c, (2 * w.rows - 1) * 32);
+    commit_into(c, d_poly, log_m, n, w.E.u32(), w.tree.u32());
+    d2h(c, w.root, w.tree.u32() + 8 * (2 * w.rows - 2), 32);
+    return w;
+}
+
+// extract_row for each query (src/ligero.rs:40-51) + merkle_tree::prove
+void open(lg_ctx *c, const Witness &w, const std::vector<uint64_t> &q, lg::Opening &out,
+          std::vector<uint32_t> &rows_flat) {
+    std::vector<NodeRef> refs;
+    lg::merkle_proof_nodes(q, w.rows, refs);
+    const size_t nq = q.size(), nr = refs.size();
+    std::vector<uint64_t> idx(nq + nr);
+    std::copy(q.begin(), q.end(), idx.begin());
+    std::vector<uint64_t> layer_off(64, 0);
+    for (uint32_t l = 1; l < 64; ++l) layer_off[l] = layer_off[l - 1] + (w.rows >> (l - 1));
+    for (size_t i = 0; i < nr; ++i) idx[nq + i] = layer_off[refs[i].layer] + refs[i].index;
+    DBuf d_idx(c, idx.size() * 8);
+    DBuf d_out(c, (nq * w.cols + nr * 8) * 4 + 16);
+    h2d(c, d_idx.p, idx.data(), idx.size() * 8);
+    CK(c, lgk::gather_rows(c->L, w.E.u32(), w.rows, w.cols, d_idx.u64(), (uint32_t)nq, d_out.u32()));
+    CK(c, lgk::gather_nodes(c->L, w.tree.u32(), d_idx.u64() + nq, (uint32_t)nr, d_out.u32() + nq * w.cols));
+    std::vector<uint32_t> host(nq * w.cols + nr * 8);
+    d2h(c, host.data(), d_out.p, host.size() * 4);
+    rows_flat.assign(host.begin(), host.begin() + nq * w.cols);
+    out.rows.resize(nq);
+    for (size_t k = 0; k < nq; ++k) out.rows[k].assign(host.begin() + k * w.cols, host.begin() + (k + 1) * w.cols);
+    out.merkle.resize(nr);
+    for (size_t i = 0; i < nr; ++i) {
+        const uint8_t *b = reinterpret_cast<const uint8_t *>(host.data() + nq * w.cols + 8 * i);
+        out.merkle[i].assign(b, b + 32);
+    }
+}
+
+// induce_sumcheck_poly_parallel (src/sumcheck_polys.rs:74-160).  The
+// enforced sum (148 dot products of one row each) is host work; the 2^n
+// basis goes to the device.
+uint32_t induce(lg_ctx *c, uint32_t n, const uint32_t *rows, size_t nrows, const uint32_t *vch, uint32_t nch,
+                const std::vector<uint64_t> &q, uint32_t alpha, uint32_t *d_out) {
+    const size_t glen = 1ull << nch;
+    std::vector<uint32_t> gr = lg::lagrange_basis(vch, nch);
+    std::vector<uint32_t> apow(nrows);
+    uint32_t sum = 0;
+    for (size_t k = 0; k < nrows; ++k) {
+        apow[k] = k ? lg::gf_mul(apow[k - 1], alpha) : 1u;
+        uint32_t dot = 0;
+        for (size_t j = 0; j < glen; ++j) dot ^= lg::gf_mul(rows[k * glen + j], gr[j]);
+        sum ^= lg::gf_mul(dot, apow[k]);
+    }
+    // sks_at_x per query (src/binary_fft.rs:276-301): S[0] = x, S[i] = next_s(S[i-1], sks[i-1])
+    std::vector<uint32_t> sks = lg::eval_sk_at_vks(1ull << n);
+    std::vector<uint32_t> S(nrows * std::max<uint32_t>(n, 1));
+    for (size_t k = 0; k < nrows; ++k) {
+        uint32_t *s = S.data() + k * n;
+        if (n == 0) continue;
+        s[0] = (uint32_t)q[k];
+        for (uint32_t i = 1; i < n; ++i) s[i] = lg::next_s(s[i - 1], sks[i - 1]);
+    }
+    lgk::InducePlan plan = lgk::induce_plan(n, (uint32_t)nrows);
+    DBuf dlo(c, nrows * (4ull << plan.b)), dhi(c, nrows * (4ull << (n - plan.b)));
+    std::vector<uint32_t> up(S);
+    up.insert(up.end(), apow.begin(), apow.end());
+    DBuf dup(c, up.size() * 4);
+    h2d(c, dup.p, up.data(), up.size() * 4);
+    if (plan.needs_zero) CK(c, cudaMemsetAsync(d_out, 0, 4ull << n, c->stream));
+    CK(c, lgk::induce_basis(c->L, plan, dup.u32(), dup.u32() + S.size(), n, (uint32_t)nrows, dlo.u32(),
+                            dhi.u32(), d_out));
+    return sum;
+}
+
+std::array<uint32_t, 3> read3(lg_ctx *c, const DBuf &acc) {
+    std::array<uint32_t, 3> s;
+    d2h(c, s.data(), acc.p, 12);
+    return s;
+}
+
+// partial_eval by any number of challenges, chunks of <= 6 per launch
+void partial_eval_dev(lg_ctx *c, const uint32_t *d_in, uint32_t log_len, const uint32_t *rs, uint32_t k,
+                      uint32_t *d_out) {
+    DBuf tmp[2];
+    const uint32_t *src = d_in;
+    uint32_t cur = log_len, done = 0, which = 0;
+    while (done < k) {
+        const uint32_t kk = std::min<uint32_t>(6, k - done);
+        std::vector<uint32_t> gr = lg::lagrange_basis(rs + done, kk);
+        uint32_t *dst;
+        if (done + kk == k) dst = d_out;
+        else {
+            tmp[which] = DBuf(c, 4ull << (cur - kk));
+            dst = tmp[which].u32();
+        }
+        CK(c, lgk::fold_eq(c->L, src, dst, cur, kk, gr.data()));
+        src = dst;
+        which ^= 1;
+        cur -= kk;
+        done += kk;
+    }
+}
+
+void absorb3(lg::Transcript &fs, const std::array<uint32_t, 3> &s) { fs.absorb_u32s(s.data(), 3); }
+
+// ------------------------------------------------------------------ prover
+// prover (src/prover.rs:15-199)
+void prove_impl(lg_ctx *c, const lg_config &cfg, const uint32_t *d_poly, uint64_t len, lg::Proof &P) {
+    const size_t s = LG_NUM_QUERIES;
+    lg::Transcript fs(LG_FS_SEED);
+    Witness w0 = commit(c, d_poly, cfg.initial_log_m, 1u << cfg.initial_log_n);  // :32-37
+    P.initial_root.assign(w0.root, w0.root + 32);
+    fs.absorb(w0.root, 32);  // :48
+
+    std::vector<uint32_t> pe0(cfg.initial_k);
+    for (auto &r : pe0) r = fs.get_field();  // :50
+    uint32_t fv = cfg.initial_log_m;         // log2 |f|
+    DBuf f(c, 4ull << fv);
+    partial_eval_dev(c, d_poly, cfg.initial_log_m + cfg.initial_log_n, pe0.data(), cfg.initial_k, f.u32());  // :52-53
+
+    Witness wprev = commit(c, f.u32(), cfg.log_m[0], 1u << cfg.log_n[0]);  // :55-60
+    fs.absorb(wprev.root, 32);                                             // :64
+    P.recursive_roots.push_back(std::vector<uint8_t>(wprev.root, wprev.root + 32));
+
+    std::vector<uint64_t> q;
+    if (!fs.get_distinct_queries(w0.rows, s, q)) throw ProverAssert{};  // :67
+    const uint32_t alpha = fs.get_field();                             // :68
+    std::vector<uint32_t> rows;
+    open(c, w0, q, P.initial, rows);  // :72-76
+    w0.E.reset();
+    w0.tree.reset();
+    DBuf B(c, 4ull << fv);
+    const uint32_t h1 = induce(c, fv, rows.data(), s, pe0.data(), cfg.initial_k, q, alpha, B.u32());  // :78-85
+
+    DBuf acc(c, 16);
+    CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
+    CK(c, lgk::eval013(c->L, f.u32(), B.u32(), fv, acc.u32()));  // SumcheckProverInstance::new
+    std::array<uint32_t, 3> s3 = read3(c, acc);
+    if ((s3[0] ^ s3[1]) != h1) throw ProverAssert{};  // src/ligerito.rs:35
+    P.transcript.push_back(s3);
+    absorb3(fs, s3);  // :93
+
+    DBuf f2(c, 4ull << (fv - 1)), B2(c, 4ull << (fv - 1));
+    for (uint32_t i = 0; i < cfg.recursive_steps; ++i) {
+        std::vector<uint32_t> rs;
+        for (uint32_t t = 0; t < cfg.ks[i]; ++t) {  // :97-102
+            const uint32_t r = fs.get_field();
+            CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
+            CK(c, lgk::fold_round(c->L, f.u32(), B.u32(), fv, r, f2.u32(), B2.u32(), acc.u32()));
+            std::swap(f, f2);
+            std::swap(B, B2);
+            fv -= 1;
+            s3 = read3(c, acc);
+            P.transcript.push_back(s3);
+            absorb3(fs, s3);
+            rs.push_back(r);
+        }
+        if (i == cfg.recursive_steps - 1) {  // :104-143
+            P.yr.resize(1ull << fv);
+            d2h(c, P.yr.data(), f.p, 4ull << fv);
+            fs.absorb_u32s(P.yr.data(), P.yr.size());
+            if (!fs.get_distinct_queries(wprev.rows, s, q)) throw ProverAssert{};
+            open(c, wprev, q, P.final_, rows);
+            return;
+        }
+        Witness wn = commit(c, f.u32(), cfg.log_m[i + 1], 1u << cfg.log_n[i + 1]);  // :145-155
+        fs.absorb(wn.root, 32);
+        P.recursive_roots.push_back(std::vector<uint8_t>(wn.root, wn.root + 32));
+        if (!fs.get_distinct_queries(wprev.rows, s, q)) throw ProverAssert{};  // :157
+        const uint32_t al = fs.get_field();                                  // :158
+        lg::Opening op;
+        open(c, wprev, q, op, rows);  // :161-172
+        P.recursive.push_back(std::move(op));
+        DBuf bi(c, 4ull << fv);
+        const uint32_t h = induce(c, fv, rows.data(), s, rs.data(), cfg.ks[i], q, al, bi.u32());  // :174-181
+        CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
+        CK(c, lgk::eval013(c->L, f.u32(), bi.u32(), fv, acc.u32()));  // introduce_new
+        s3 = read3(c, acc);
+        if ((s3[0] ^ s3[1]) != h) throw ProverAssert{};  // src/ligerito.rs:52
+        P.transcript.push_back(s3);
+        absorb3(fs, s3);  // :187-191
+        const uint32_t beta = fs.get_field();  // :193
+        CK(c, lgk::axpy(c->L, B.u32(), bi.u32(), fv, beta));  // glue
+        wprev = std::move(wn);
+    }
+    throw ProverAssert{};  // :198
+}
+
+// ---------------------------------------------------------------- verifier
+struct Quad { uint32_t a, b, c; };  // QuadraticPoly, src/sumcheck.rs:38-65
+Quad quad_from_evals(uint32_t at0, uint32_t at1, uint32_t atx) {  // :67-81, x = 3
+    const uint32_t x = 3;
+    static const uint32_t inv_den = lg::gf_inv(lg::gf_mul(x, x) ^ x);
+    const uint32_t num = atx ^ at0 ^ lg::gf_mul(x, at1 ^ at0);
+    const uint32_t a = lg::gf_mul(num, inv_den);
+    return {a, at1 ^ at0 ^ a, at0};
+}
+uint32_t eval_quad(const Quad &p, uint32_t r) { return lg::gf_mul(lg::gf_mul(p.a, r), r) ^ lg::gf_mul(p.b, r) ^ p.c; }
+
+// merkle_tree::verify of an opening (leaf bytes = LE words of each row)
+bool opening_ok(const std::vector<uint8_t> &root, const lg::Opening &o, size_t depth,
+                const std::vector<uint64_t> &q) {
+    if (o.rows.size() < q.size()) return false;  // layer index panic
+    std::vector<std::array<uint8_t, 32>> layer(q.size());
+    std::vector<uint8_t> buf;
+    for (size_t i = 0; i < q.size(); ++i) {
+        buf.resize(4 * o.rows[i].size());
+        for (size_t j = 0; j < o.rows[i].size(); ++j) {
+            uint32_t v = o.rows[i][j];
+            buf[4 * j] = (uint8_t)v; buf[4 * j + 1] = (uint8_t)(v >> 8);
+            buf[4 * j + 2] = (uint8_t)(v >> 16); buf[4 * j + 3] = (uint8_t)(v >> 24);
+        }
+        lg::blake3_hash(buf.data(), buf.size(), layer[i].data());
+    }
+    bool ok = false;
+    if (!lg::merkle_verify(root.data(), root.size(), o.merkle, depth, layer, q, &ok)) return false;
+    return ok;
+}
+
+std::vector<uint32_t> dense(const lg::Opening &o, size_t want_rows, size_t want_len) {
+    if (o.rows.size() != want_rows) throw VerifyPanic{};  // assert_eq (src/sumcheck_polys.rs:98)
+    std::vector<uint32_t> r(want_rows * want_len);
+    for (size_t k = 0; k < want_rows; ++k) {
+        if (o.rows[k].size() != want_len) throw VerifyPanic{};  // :97
+        std::copy(o.rows[k].begin(), o.rows[k].end(), r.begin() + k * want_len);
+    }
+    return r;
+}
+
+// ligero_verify (src/ligero.rs:97-131); rows zip against gr (truncation)
+void ligero_verify_host(const std::vector<uint64_t> &q, const lg::Opening &o, const std::vector<uint32_t> &yr,
+                        const std::vector<uint32_t> &ch) {
+    std::vector<uint32_t> gr = lg::lagrange_basis(ch.data(), ch.size());
+    const size_t ylen = yr.size();
+    if (ylen == 0 || (ylen & (ylen - 1))) throw VerifyPanic{};
+    uint32_t nv = 0;
+    while ((1ull << nv) < ylen) ++nv;
+    std::vector<uint32_t> sks = lg::eval_sk_at_vks(ylen), basis(ylen), sx(nv + 1);
+    if (o.rows.size() > q.size()) throw VerifyPanic{};
+    for (size_t i = 0; i < o.rows.size(); ++i) {
+        uint32_t dot = 0;
+        const size_t zl = std::min(o.rows[i].size(), gr.size());
+        for (size_t j = 0; j < zl; ++j) dot ^= lg::gf_mul(o.rows[i][j], gr[j]);
+        if (q[i] > 0xFFFFFFFFull) throw VerifyPanic{};
+        sx[0] = (uint32_t)q[i];
+        for (uint32_t t = 1; t < nv; ++t) sx[t] = lg::next_s(sx[t - 1], sks[t - 1]);
+        basis[0] = 1;
+        for (uint32_t t = 0; t < nv; ++t) {
+            const size_t cur = 1ull << t;
+            for (size_t j = 0; j < cur; ++j) basis[cur + j] = lg::gf_mul(sx[t], basis[j]);
+        }
+        uint32_t e = 0;
+        for (size_t j = 0; j < ylen; ++j) e ^= lg::gf_mul(yr[j], basis[j]);
+        if (e != dot) throw VerifyPanic{};
+    }
+}
+
+bool verify_impl(lg_ctx *c, const lg_config &cfg, const lg::Proof &P) {
+    const size_t s = LG_NUM_QUERIES;
+    const uint32_t log_inv_rate = 2;  // src/verifier.rs:26
+    lg::Transcript fs(LG_FS_SEED);
+    fs.absorb(P.initial_root.data(), P.initial_root.size());  // :27
+    std::vector<uint32_t> pe0(cfg.initial_k);
+    for (auto &r : pe0) r = fs.get_field();  // :29
+    if (P.recursive_roots.empty()) throw VerifyPanic{};
+    fs.absorb(P.recursive_roots[0].data(), P.recursive_roots[0].size());  // :30
+    size_t depth = cfg.initial_log_m + log_inv_rate;
+    std::vector<uint64_t> q;
+    if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};
+    if (!opening_ok(P.initial_root, P.initial, depth, q)) throw VerifyPanic{};  // :42-49
+    const uint32_t alpha = fs.get_field();
+    std::vector<uint32_t> rows = dense(P.initial, s, 1ull << cfg.initial_k);
+    std::vector<DBuf> basis;
+    std::vector<uint32_t> bvars, sep;
+    basis.emplace_back(c, 4ull << cfg.initial_log_m);
+    bvars.push_back(cfg.initial_log_m);
+    sep.push_back(1);
+    const uint32_t h1 = induce(c, cfg.initial_log_m, rows.data(), s, pe0.data(), cfg.initial_k, q, alpha,
+                               basis.back().u32());  // :53-60
+    // SumcheckVerifierInstance::new (src/ligerito.rs:172-192)
+    size_t rd = 0;
+    auto read_tr = [&]() {
+        if (rd >= P.transcript.size()) throw VerifyPanic{};
+        return P.transcript[rd++];
+    };
+    std::array<uint32_t, 3> g = read_tr();
+    if ((g[0] ^ g[1]) != h1) throw VerifyPanic{};
+    Quad running = quad_from_evals(g[0], g[1], g[2]);
+    absorb3(fs, g);  // :67
+    std::vector<uint32_t> ris;
+    for (uint32_t i = 0; i < cfg.recursive_steps; ++i) {
+        std::vector<uint32_t> rs;
+        for (uint32_t t = 0; t < cfg.ks[i]; ++t) {  // :70-76, fold :201-210
+            const uint32_t r = fs.get_field();
+            ris.push_back(r);
+            const uint32_t sum = eval_quad(running, r);
+            g = read_tr();
+            if ((g[0] ^ g[1]) != sum) throw VerifyPanic{};
+            running = quad_from_evals(g[0], g[1], g[2]);
+            absorb3(fs, g);
+            rs.push_back(r);
+        }
+        if (i >= P.recursive_roots.size()) throw VerifyPanic{};
+        const std::vector<uint8_t> &root = P.recursive_roots[i];
+        if (i == cfg.recursive_steps - 1) {  // :78-120
+            fs.absorb_u32s(P.yr.data(), P.yr.size());
+            depth = cfg.log_m[i] + log_inv_rate;
+            if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};
+            if (!opening_ok(root, P.final_, depth, q)) throw VerifyPanic{};
+            ligero_verify_host(q, P.final_, P.yr, rs);
+            const uint32_t final_r = fs.get_field();  // :114
+            const size_t yl = P.yr.size();
+            if (yl < 2) throw VerifyPanic{};
+            std::vector<uint32_t> fe(yl / 2);
+            for (size_t j = 0; j < yl / 2; ++j)
+                fe[j] = P.yr[j] ^ lg::gf_mul(final_r, P.yr[j] ^ P.yr[yl / 2 + j]);
+            // verify_partial (src/ligerito.rs:282-295)
+            uint32_t k = 0;
+            while ((1ull << k) < fe.size()) ++k;
+            const uint32_t sum = eval_quad(running, final_r);
+            ris.push_back(final_r);
+            std::vector<uint32_t> acc(fe.size(), 0), part(fe.size());
+            for (size_t bi = 0; bi < basis.size(); ++bi) {  // evaluate_basis_polys_partially :257-280
+                const uint32_t nv = bvars[bi];
+                size_t npts, first;
+                if (bi == 0) { npts = ris.size(); first = 0; }
+                else {
+                    if (nv < k || nv - k > ris.size()) throw VerifyPanic{};
+                    npts = nv - k;
+                    first = ris.size() - npts;
+                }
+                if (npts == 0 || npts > nv || (1ull << (nv - npts)) != fe.size()) throw VerifyPanic{};
+                DBuf d(c, 4ull << (nv - npts));
+                partial_eval_dev(c, basis[bi].u32(), nv, ris.data() + first, (uint32_t)npts, d.u32());
+                d2h(c, part.data(), d.p, 4 * part.size());
+                for (size_t j = 0; j < acc.size(); ++j)
+                    acc[j] ^= bi == 0 ? part[j] : lg::gf_mul(sep[bi], part[j]);
+            }
+            uint32_t dot = 0;
+            for (size_t j = 0; j < fe.size(); ++j) dot ^= lg::gf_mul(fe[j], acc[j]);
+            return dot == sum;
+        }
+        if (i + 1 >= P.recursive_roots.size() || i >= P.recursive.size()) throw VerifyPanic{};
+        fs.absorb(P.recursive_roots[i + 1].data(), P.recursive_roots[i + 1].size());  // :122
+        depth = cfg.log_m[i] + log_inv_rate;
+        if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};  // :126
+        if (!opening_ok(root, P.recursive[i], depth, q)) throw VerifyPanic{};
+        const uint32_t al = fs.get_field();  // :345
+        std::vector<uint32_t> rr = dense(P.recursive[i], s, 1ull << cfg.ks[i]);
+        basis.emplace_back(c, 4ull << cfg.log_m[i]);
+        bvars.push_back(cfg.log_m[i]);
+        const uint32_t h = induce(c, cfg.log_m[i], rr.data(), s, rs.data(), cfg.ks[i], q, al, basis.back().u32());
+        g = read_tr();  // introduce_new (src/ligerito.rs:212-220)
+        if ((g[0] ^ g[1]) != h) throw VerifyPanic{};
+        Quad to_glue = quad_from_evals(g[0], g[1], g[2]);
+        absorb3(fs, g);
+        const uint32_t beta = fs.get_field();  // :358
+        sep.push_back(beta);                   // glue (src/ligerito.rs:222-232)
+        running.a ^= lg::gf_mul(beta, to_glue.a);
+        running.b ^= lg::gf_mul(beta, to_glue.b);
+        running.c ^= lg::gf_mul(beta, to_glue.c);
+    }
+    throw VerifyPanic{};  // :362
+}
+
+template <class F>
+lg_status guarded(lg_ctx *c, F &&f) {
+    try {
+        f();
+        return LG_OK;
+    } catch (const CudaFail &) {
+        return LG_ERR_CUDA;
+    } catch (const OutOfBudget &) {
+        return LG_ERR_OUT_OF_MEMORY;
+    } catch (const ProverAssert &) {
+        if (c) c->err = "prover assertion failed";
+        return LG_ERR_PROVER_ASSERT;
+    } catch (const VerifyPanic &) {
+        if (c) c->err = "verifier panic";
+        return LG_ERR_VERIFY_PANIC;
+    } catch (const BadConfig &) {
+        return LG_ERR_INVALID_CONFIG;
+    } catch (const std::bad_alloc &) {
+        if (c) c->err = "host allocation failed";
+        return LG_ERR_OUT_OF_MEMORY;
+    }
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+const char *lg_status_string(lg_status s) {
+    switch (s) {
+        case LG_OK: return "ok";
+        case LG_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case LG_ERR_INVALID_CONFIG: return "invalid config";
+        case LG_ERR_OUT_OF_MEMORY: return "out of memory";
+        case LG_ERR_CUDA: return "CUDA error";
+        case LG_ERR_VERIFY_PANIC: return "verifier panic";
+        case LG_ERR_PROVER_ASSERT: return "prover assertion failed";
+        case LG_ERR_NO_DEVICE: return "no CUDA device";
+        case LG_ERR_MALFORMED_PROOF: return "malformed proof";
+    }
+    return "unknown status";
+}
+
+uint32_t lg_abi_version(void) { return LG_ABI_VERSION; }
+
+lg_status lg_hardcoded_config_20(lg_config *out) {
+    if (!out) return LG_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof *out);
+    out->recursive_steps = 1;  // src/config.rs:19-28
+    out->initial_log_m = 14;
+    out->initial_log_n = 6;
+    out->initial_k = 6;
+    out->log_m[0] = 10;
+    out->log_n[0] = 4;
+    out->ks[0] = 4;
+    return LG_OK;
+}
+
+lg_status lg_hardcoded_config_24(lg_config *out) {
+    if (!out) return LG_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof *out);
+    out->recursive_steps = 2;  // src/config.rs:82-93
+    out->initial_log_m = 18;
+    out->initial_log_n = 6;
+    out->initial_k = 6;
+    out->log_m[0] = 14; out->log_n[0] = 4; out->ks[0] = 4;
+    out->log_m[1] = 10; out->log_n[1] = 4; out->ks[1] = 4;
+    return LG_OK;
+}
+
+lg_status lg_config_make(uint32_t L, lg_config *out) {
+    if (!out || L < 16 || L > 30) return LG_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof *out);
+    out->initial_log_m = L - 6;
+    out->initial_log_n = 6;
+    out->initial_k = 6;
+    uint32_t d = L - 6, s = 0;
+    while (d - 4 >= 10 && s < LG_MAX_STEPS) {
+        out->log_m[s] = d - 4; out->log_n[s] = 4; out->ks[s] = 4;
+        ++s;
+        d -= 4;
+    }
+    if (s == 0) { out->log_m[0] = L - 10; out->log_n[0] = 4; out->ks[0] = 4; s = 1; }
+    out->recursive_steps = s;
+    return LG_OK;
+}
+
+lg_status lg_config_validate(const lg_config *cfg, uint64_t poly_len) {
+    if (!cfg) return LG_ERR_INVALID_ARGUMENT;
+    return lg::config_check(*cfg, poly_len);
+}
+
+lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
+    if (!out) return LG_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return LG_ERR_NO_DEVICE; }
+    if (device < 0 || device >= n) return LG_ERR_INVALID_ARGUMENT;
+    auto *c = new (std::nothrow) lg_ctx;
+    if (!c) return LG_ERR_OUT_OF_MEMORY;
+    c->device = device;
+    c->budget = budget;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault) != cudaSuccess) {
+        delete c;
+        return LG_ERR_CUDA;
+    }
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    c->L.stream = c->stream;
+    *out = c;
+    return LG_OK;
+}
+
+void lg_ctx_destroy(lg_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto &kv : c->codes) { cudaFree(kv.second.tw); cudaFree(kv.second.pis); }
+    for (auto &kv : c->ffttw) cudaFree(kv.second);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    c->L.release();
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *lg_ctx_last_error(const lg_ctx *c) { return c ? c->err.c_str() : "null context"; }
+void *lg_ctx_stream(lg_ctx *c) { return c ? (void *)c->stream : nullptr; }
+lg_status lg_ctx_synchronize(lg_ctx *c) {
+    if (!c) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] { sync(c); });
+}
+uint64_t lg_ctx_launch_count(const lg_ctx *c) { return c ? c->L.launches : 0; }
+lg_status lg_ctx_set_kernel_timing(lg_ctx *c, int on) {
+    if (!c) return LG_ERR_INVALID_ARGUMENT;
+    c->L.timing = on != 0;
+    return LG_OK;
+}
+lg_status lg_ctx_kernel_stats(lg_ctx *c, uint32_t index, char *name, size_t cap, uint64_t *launches, double *ms) {
+    if (!c) return LG_ERR_INVALID_ARGUMENT;
+    lg_status st = guarded(c, [&] { sync(c); c->L.resolve(); });
+    if (st != LG_OK) return st;
+    if (index >= c->L.stats.size()) return LG_ERR_INVALID_ARGUMENT;
+    auto it = c->L.stats.begin();
+    std::advance(it, index);
+    if (name && cap) { std::snprintf(name, cap, "%s", it->first.c_str()); }
+    if (launches) *launches = it->second.first;
+    if (ms) *ms = it->second.second;
+    return LG_OK;
+}
+lg_status lg_ctx_reset_kernel_stats(lg_ctx *c) {
+    if (!c) return LG_ERR_INVALID_ARGUMENT;
+    lg_status st = guarded(c, [&] { sync(c); c->L.resolve(); });
+    c->L.stats.clear();
+    return st;
+}
+uint64_t lg_ctx_device_bytes_in_use(const lg_ctx *c) { return c ? c->in_use : 0; }
+
+lg_status lg_prove(lg_ctx *c, const lg_config *cfg, const uint32_t *poly, uint64_t len, int on_device,
+                   lg_proof **out) {
+    if (!c || !cfg || !poly || !out) return LG_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    lg_status st = lg::config_check(*cfg, len);
+    if (st != LG_OK) return st;
+    auto *res = new (std::nothrow) lg_proof;
+    if (!res) return LG_ERR_OUT_OF_MEMORY;
+    st = guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        if (on_device) {
+            prove_impl(c, *cfg, poly, len, res->p);
+        } else {
+            DBuf d(c, len * 4);
+            CK(c, cudaMemcpyAsync(d.p, poly, len * 4, cudaMemcpyHostToDevice, c->stream));
+            prove_impl(c, *cfg, d.u32(), len, res->p);
+        }
+        sync(c);
+    });
+    if (st != LG_OK) { delete res; return st; }
+    *out = res;
+    return LG_OK;
+}
+
+lg_status lg_verify(lg_ctx *c, const lg_config *cfg, const lg_proof *proof, int *accepted) {
+    if (!c || !cfg || !proof || !accepted) return LG_ERR_INVALID_ARGUMENT;
+    *accepted = 0;
+    if (cfg->recursive_steps < 1 || cfg->recursive_steps > LG_MAX_STEPS || cfg->initial_k > 8 ||
+        cfg->initial_log_m > 26)
+        return LG_ERR_INVALID_CONFIG;
+    for (uint32_t i = 0; i < cfg->recursive_steps; ++i)
+        if (cfg->ks[i] > 8 || cfg->log_m[i] > 26) return LG_ERR_INVALID_CONFIG;
+    bool ok = false;
+    lg_status st = guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        ok = verify_impl(c, *cfg, proof->p);
+        sync(c);
+    });
+    if (st == LG_OK) *accepted = ok ? 1 : 0;
+    return st;
+}
+
+lg_status lg_proof_serialize(const lg_proof *p, uint8_t *buf, uint64_t *len) {
+    if (!p || !len) return LG_ERR_INVALID_ARGUMENT;
+    std::vector<uint8_t> b = lg::serialize(p->p);
+    if (!buf) { *len = b.size(); return LG_OK; }
+    if (*len < b.size()) { *len = b.size(); return LG_ERR_INVALID_ARGUMENT; }
+    std::memcpy(buf, b.data(), b.size());
+    *len = b.size();
+    return LG_OK;
+}
+
+lg_status lg_proof_deserialize(const uint8_t *buf, uint64_t len, lg_proof **out) {
+    if (!buf || !out) return LG_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    auto *p = new (std::nothrow) lg_proof;
+    if (!p) return LG_ERR_OUT_OF_MEMORY;
+    if (!lg::deserialize(buf, len, p->p)) { delete p; return LG_ERR_MALFORMED_PROOF; }
+    *out = p;
+    return LG_OK;
+}
+
+void lg_proof_free(lg_proof *p) { delete p; }
+
+lg_status lg_proof_size(const lg_proof *p, uint64_t *bytes) {
+    if (!p || !bytes) return LG_ERR_INVALID_ARGUMENT;
+    *bytes = lg::proof_size(p->p);
+    return LG_OK;
+}
+
+lg_status lg_compute_twiddles(uint32_t log_n, uint32_t *out) {
+    if (!out || log_n < 1 || log_n > 30) return LG_ERR_INVALID_ARGUMENT;
+    lg::compute_twiddles(log_n, out);
+    return LG_OK;
+}
+
+static lg_status fft_common(lg_ctx *c, uint32_t *d, uint32_t log_n, uint64_t batch, bool inv) {
+    if (!c || !d || log_n < 1 || log_n > 30 || batch == 0 || batch > 0xFFFFFFFFull) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        const uint32_t *tw = get_fft_tw(c, log_n);
+        CK(c, lgk::fft_vectors(c->L, d, tw, log_n, (uint32_t)batch, 1ull << log_n, 1, 0, 1, inv));
+        sync(c);
+    });
+}
+lg_status lg_fft(lg_ctx *c, uint32_t *d, uint32_t log_n, uint64_t batch) { return fft_common(c, d, log_n, batch, false); }
+lg_status lg_ifft(lg_ctx *c, uint32_t *d, uint32_t log_n, uint64_t batch) { return fft_common(c, d, log_n, batch, true); }
+
+lg_status lg_rs_encode_cols(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *d_enc) {
+    if (!c || !d_poly || !d_enc || log_m < 1 || log_m > 26 || n == 0) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        const Code &code = get_code(c, log_m);
+        CK(c, lgk::rs_scale_spread(c->L, d_poly, code.pis, d_enc, log_m, n));
+        CK(c, lgk::fft_vectors(c->L, d_enc, code.tw, log_m, n, 4ull << log_m, 4, 1ull << log_m, 4, false));
+        sync(c);
+    });
+}
+
+lg_status lg_ligero_commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *d_enc,
+                           uint8_t *d_tree, uint8_t *root) {
+    if (!c || !d_poly || !d_enc || !d_tree || log_m < 1 || log_m > 26 || n == 0 || n > 256)
+        return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        commit_into(c, d_poly, log_m, n, d_enc, reinterpret_cast<uint32_t *>(d_tree));
+        const uint64_t rows = 4ull << log_m;
+        if (root) d2h(c, root, d_tree + 32 * (2 * rows - 2), 32);
+        sync(c);
+    });
+}
+
+lg_status lg_partial_eval(lg_ctx *c, const uint32_t *d_evals, uint32_t log_len, const uint32_t *rs, uint32_t k,
+                          uint32_t *d_out) {
+    if (!c || !d_evals || !rs || !d_out || k == 0 || k > log_len || log_len > 34) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        partial_eval_dev(c, d_evals, log_len, rs, k, d_out);
+        sync(c);
+    });
+}
+
+lg_status lg_eval_013_product(lg_ctx *c, const uint32_t *d_f, const uint32_t *d_g, uint32_t log_len, uint32_t out[3]) {
+    if (!c || !d_f || !d_g || !out || log_len < 1 || log_len > 34) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        DBuf acc(c, 16);
+        CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
+        CK(c, lgk::eval013(c->L, d_f, d_g, log_len, acc.u32()));
+        std::array<uint32_t, 3> s = read3(c, acc);
+        out[0] = s[0]; out[1] = s[1]; out[2] = s[2];
+    });
+}
+
+lg_status lg_induce_sumcheck_poly(lg_ctx *c, uint32_t n, const uint32_t *rows, uint32_t nrows, const uint32_t *vch,
+                                  uint32_t nch, const uint64_t *queries, uint32_t alpha, uint32_t *d_out,
+                                  uint32_t *enforced_sum) {
+    if (!c || !rows || !vch || !queries || !d_out || !enforced_sum || nch == 0 || nch > 8 || n > 28 || nrows == 0)
+        return LG_ERR_INVALID_ARGUMENT;
+    for (uint32_t k = 0; k < nrows; ++k)
+        if (queries[k] > 0xFFFFFFFFull) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        std::vector<uint64_t> q(queries, queries + nrows);
+        *enforced_sum = induce(c, n, rows, nrows, vch, nch, q, alpha, d_out);
+        sync(c);
+    });
+}
+
+struct lg_transcript {
+    lg::Transcript t;
+    explicit lg_transcript(uint32_t seed) : t(seed) {}
+};
+
+lg_status lg_transcript_new(uint32_t seed, lg_transcript **out) {
+    if (!out) return LG_ERR_INVALID_ARGUMENT;
+    *out = new (std::nothrow) lg_transcript(seed);
+    return *out ? LG_OK : LG_ERR_OUT_OF_MEMORY;
+}
+void lg_transcript_free(lg_transcript *t) { delete t; }
+lg_status lg_transcript_absorb(lg_transcript *t, const uint8_t *b, uint64_t len) {
+    if (!t || (!b && len)) return LG_ERR_INVALID_ARGUMENT;
+    t->t.absorb(b, len);
+    return LG_OK;
+}
+lg_status lg_transcript_squeeze(lg_transcript *t, uint64_t out[2]) {
+    if (!t || !out) return LG_ERR_INVALID_ARGUMENT;
+    auto v = t->t.squeeze();
+    out[0] = v[0];
+    out[1] = v[1];
+    return LG_OK;
+}
+lg_status lg_transcript_get_field(lg_transcript *t, uint32_t *out) {
+    if (!t || !out) return LG_ERR_INVALID_ARGUMENT;
+    *out = t->t.get_field();
+    return LG_OK;
+}
+lg_status lg_transcript_get_query(lg_transcript *t, uint64_t n, uint64_t *out) {
+    if (!t || !out || n == 0) return LG_ERR_INVALID_ARGUMENT;
+    *out = t->t.get_query(n);
+    return LG_OK;
+}
+lg_status lg_transcript_get_distinct_queries(lg_transcript *t, uint64_t n, uint64_t s, uint64_t *out) {
+    if (!t || (!out && s)) return LG_ERR_INVALID_ARGUMENT;
+    std::vector<uint64_t> q;
+    if (!t->t.get_distinct_queries(n, s, q)) return LG_ERR_INVALID_ARGUMENT;
+    std::copy(q.begin(), q.end(), out);
+    return LG_OK;
+}
+
+lg_status lg_merkle_verify(const uint8_t *root, const uint8_t *proof, uint64_t n_sib, uint64_t depth,
+                           const uint8_t *leaves, const uint64_t *off, const uint64_t *queries, uint64_t nq,
+                           int *ok) {
+    if (!root || !ok || (!proof && n_sib) || (nq && (!leaves || !off || !queries)) || depth > 64)
+        return LG_ERR_INVALID_ARGUMENT;
+    std::vector<std::array<uint8_t, 32>> layer(nq);
+    for (uint64_t i = 0; i < nq; ++i) lg::blake3_hash(leaves + off[i], off[i + 1] - off[i], layer[i].data());
+    std::vector<std::vector<uint8_t>> sib(n_sib);
+    for (uint64_t i = 0; i < n_sib; ++i) sib[i].assign(proof + 32 * i, proof + 32 * i + 32);
+    bool good = false;
+    if (!lg::merkle_verify(root, 32, sib, depth, layer, std::vector<uint64_t>(queries, queries + nq), &good)) {
+        *ok = 0;
+        return LG_ERR_VERIFY_PANIC;
+    }
+    *ok = good ? 1 : 0;
+    return LG_OK;
+}
+
+lg_status lg_fill_splitmix(lg_ctx *c, uint64_t seed, uint32_t *d_out, uint64_t n) {
+    if (!c || !d_out) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        CK(c, lgk::splitmix(c->L, seed, d_out, n));
+        sync(c);
+    });
+}
+
+void lg_fill_splitmix_host(uint64_t seed, uint32_t *out, uint64_t n) {
+    if (out) lg::splitmix_fill(seed, out, n, 0);
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// Device primitives for liblgpu (sm_100a): GF(2^32) arithmetic and BLAKE3.
+//
+// GF(2^32) = GF(2)[x] / (x^32 + x^15 + x^9 + x^7 + x^4 + x^3 + 1), the
+// polynomial basis of src/binary_field.rs:179-181.  There is no carry-less
+// multiply instruction, so two forms are used:
+//   * gf_mul(a, b): a general product from 16 32x32->64 integer multiplies
+//     of operands masked to every 4th bit (each partial-product coefficient
+//     is a count <= 8 < 16, so the integer sums never carry into the next
+//     4-bit lane), XOR-combined and reduced.
+//   * MulTab: a per-constant table of c * e * x^(w*B) for every B-bit window
+//     value e; c * v is then the XOR of one table word per window of v.
+//     Warps look a constant's table up together, so all lanes read one
+//     32-word bank row (conflict-free).  Used wherever many products share a
+//     multiplier: FFT twiddles (shared across all matrix columns), fold
+//     challenges, sumcheck challenges, basis-expansion constants.
+#pragma once
+#include <cstdint>
+
+namespace lgd {
+
+constexpr uint32_t kTail = 0x8299u;  // x^32 mod p
+
+__device__ __forceinline__ uint32_t red_small(uint32_t t) {
+    // t * (x^15 + x^9 + x^7 + x^4 + x^3 + 1) for deg t <= 16 (no overflow)
+    return t ^ (t << 3) ^ (t << 4) ^ (t << 7) ^ (t << 9) ^ (t << 15);
+}
+
+__device__ __forceinline__ uint32_t gf_mulx(uint32_t a) {
+    return (a << 1) ^ ((uint32_t)((int32_t)a >> 31) & kTail);
+}
+// a * x^k for 1 <= k <= 16
+template <int K>
+__device__ __forceinline__ uint32_t gf_mulxk(uint32_t a) {
+    return (a << K) ^ red_small(a >> (32 - K));
+}
+
+__device__ __forceinline__ uint32_t gf_reduce(uint32_t hi, uint32_t lo) {
+    uint32_t lo2 = hi ^ (hi << 3) ^ (hi << 4) ^ (hi << 7) ^ (hi << 9) ^ (hi << 15);
+    uint32_t ov = (hi >> 29) ^ (hi >> 28) ^ (hi >> 25) ^ (hi >> 23) ^ (hi >> 17);
+    return lo ^ lo2 ^ red_small(ov);
+}
+
+__device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
+    const uint32_t m0 = 0x11111111u, m1 = 0x22222222u, m2 = 0x44444444u, m3 = 0x88888888u;
+    uint32_t a0 = a & m0, a1 = a & m1, a2 = a & m2, a3 = a & m3;
+    uint32_t b0 = b & m0, b1 = b & m1, b2 = b & m2, b3 = b & m3;
+    uint64_t z0 = ((uint64_t)a0 * b0) ^ ((uint64_t)a1 * b3) ^ ((uint64_t)a2 * b2) ^ ((uint64_t)a3 * b1);
+    uint64_t z1 = ((uint64_t)a0 * b1) ^ ((uint64_t)a1 * b0) ^ ((uint64_t)a2 * b3) ^ ((uint64_t)a3 * b2);
+    uint64_t z2 = ((uint64_t)a0 * b2) ^ ((uint64_t)a1 * b1) ^ ((uint64_t)a2 * b0) ^ ((uint64_t)a3 * b3);
+    uint64_t z3 = ((uint64_t)a0 * b3) ^ ((uint64_t)a1 * b2) ^ ((uint64_t)a2 * b1) ^ ((uint64_t)a3 * b0);
+    uint64_t r = (z0 & 0x1111111111111111ull) | (z1 & 0x2222222222222222ull) |
+                 (z2 & 0x4444444444444444ull) | (z3 & 0x8888888888888888ull);
+    return gf_reduce((uint32_t)(r >> 32), (uint32_t)r);
+}
+
+// ---------------------------------------------------------------- MulTab
+// 4-bit windows: 8 windows x 16 entries = 128 words (512 B) per constant.
+constexpr int kTabWords = 128;
+
+// One warp builds the table of constant c (all 32 lanes participate).
+__device__ __forceinline__ void tab_build_warp(uint32_t *T, uint32_t c, int lane) {
+    uint32_t c1 = gf_mulx(c), c2 = gf_mulx(c1), c3 = gf_mulx(c2);
+    int e = lane & 15;
+    uint32_t v = ((e & 1) ? c : 0u) ^ ((e & 2) ? c1 : 0u) ^ ((e & 4) ? c2 : 0u) ^ ((e & 8) ? c3 : 0u);
+    if (lane & 16) v = gf_mulxk<4>(v);
+    T[lane] = v;
+    v = gf_mulxk<8>(v);
+    T[32 + lane] = v;
+    v = gf_mulxk<8>(v);
+    T[64 + lane] = v;
+    v = gf_mulxk<8>(v);
+    T[96 + lane] = v;
+}
+
+// c * w, with T the table of c
+__device__ __forceinline__ uint32_t tab_mul(const uint32_t *__restrict__ T, uint32_t w) {
+    uint32_t r0 = T[w & 15u] ^ T[16 + ((w >> 4) & 15u)];
+    uint32_t r1 = T[32 + ((w >> 8) & 15u)] ^ T[48 + ((w >> 12) & 15u)];
+    uint32_t r2 = T[64 + ((w >> 16) & 15u)] ^ T[80 + ((w >> 20) & 15u)];
+    uint32_t r3 = T[96 + ((w >> 24) & 15u)] ^ T[112 + (w >> 28)];
+    return (r0 ^ r1) ^ (r2 ^ r3);
+}
+
+// ---------------------------------------------------------------- BLAKE3
+// BLAKE3 compression (BLAKE3 specification; the reference calls the blake3
+// crate, src/merkle_tree.rs:15,50).  Message schedule unrolled at compile
+// time; rotations by 16/8 are byte permutes, 12/7 funnel shifts.
+enum : uint32_t { B3_CHUNK_START = 1, B3_CHUNK_END = 2, B3_ROOT = 8 };
+
+__device__ __forceinline__ uint32_t rotr16(uint32_t x) { return __byte_perm(x, 0, 0x1032); }
+__device__ __forceinline__ uint32_t rotr8(uint32_t x) { return __byte_perm(x, 0, 0x0321); }
+__device__ __forceinline__ uint32_t rotr12(uint32_t x) { return __funnelshift_r(x, x, 12); }
+__device__ __forceinline__ uint32_t rotr7(uint32_t x) { return __funnelshift_r(x, x, 7); }
+
+#define LGD_B3G(a, b, c, d, x, y)          \
+    a = a + b + (x); d = rotr16(d ^ a);    \
+    c = c + d;       b = rotr12(b ^ c);    \
+    a = a + b + (y); d = rotr8(d ^ a);     \
+    c = c + d;       b = rotr7(b ^ c);
+
+// Message schedule: entry (r, i) is the message word at position i of
+// round r, i.e. the spec's permutation applied r times, as compile-time
+// constants so the message words stay in registers.
+#define LGD_S(r, i) (B3SchedC<r, i>::value)
+template <int R, int I> struct B3SchedC;
+#define LGD_DEF_ROW(r, a0, a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15) \
+    template <> struct B3SchedC<r, 0> { static constexpr int value = a0; };                 \
+    template <> struct B3SchedC<r, 1> { static constexpr int value = a1; };                 \
+    template <> struct B3SchedC<r, 2> { static constexpr int value = a2; };                 \
+    template <> struct B3SchedC<r, 3> { static constexpr int value = a3; };                 \
+    template <> struct B3SchedC<r, 4> { static constexpr int value = a4; };                 \
+    template <> struct B3SchedC<r, 5> { static constexpr int value = a5; };                 \
+    template <> struct B3SchedC<r, 6> { static constexpr int value = a6; };                 \
+    template <> struct B3SchedC<r, 7> { static constexpr int value = a7; };                 \
+    template <> struct B3SchedC<r, 8> { static constexpr int value = a8; };                 \
+    template <> struct B3SchedC<r, 9> { static constexpr int value = a9; };                 \
+    template <> struct B3SchedC<r, 10> { static constexpr int value = a10; };               \
+    template <> struct B3SchedC<r, 11> { static constexpr int value = a11; };               \
+    template <> struct B3SchedC<r, 12> { static constexpr int value = a12; };               \
+    template <> struct B3SchedC<r, 13> { static constexpr int value = a13; };               \
+    template <> struct B3SchedC<r, 14> { static constexpr int value = a14; };               \
+    template <> struct B3SchedC<r, 15> { static constexpr int value = a15; };
+LGD_DEF_ROW(0, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15)
+LGD_DEF_ROW(1, 2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8)
+LGD_DEF_ROW(2, 3, 4, 10, 12, 13, 2, 7, 14, 6, 5, 9, 0, 11, 15, 8, 1)
+LGD_DEF_ROW(3, 10, 7, 12, 9, 14, 3, 13, 15, 4, 0, 11, 2, 5, 8, 1, 6)
+LGD_DEF_ROW(4, 12, 13, 9, 11, 15, 10, 14, 8, 7, 2, 5, 3, 0, 1, 6, 4)
+LGD_DEF_ROW(5, 9, 14, 11, 5, 8, 12, 15, 1, 13, 3, 0, 10, 2, 6, 4, 7)
+LGD_DEF_ROW(6, 11, 15, 5, 0, 1, 9, 8, 6, 14, 10, 2, 12, 3, 4, 7, 13)
+#undef LGD_DEF_ROW
+
+template <int R>
+__device__ __forceinline__ void b3_round(uint32_t (&v)[16], const uint32_t (&m)[16]) {
+    LGD_B3G(v[0], v[4], v[8], v[12], m[LGD_S(R, 0)], m[LGD_S(R, 1)])
+    LGD_B3G(v[1], v[5], v[9], v[13], m[LGD_S(R, 2)], m[LGD_S(R, 3)])
+    LGD_B3G(v[2], v[6], v[10], v[14], m[LGD_S(R, 4)], m[LGD_S(R, 5)])
+    LGD_B3G(v[3], v[7], v[11], v[15], m[LGD_S(R, 6)], m[LGD_S(R, 7)])
+    LGD_B3G(v[0], v[5], v[10], v[15], m[LGD_S(R, 8)], m[LGD_S(R, 9)])
+    LGD_B3G(v[1], v[6], v[11], v[12], m[LGD_S(R, 10)], m[LGD_S(R, 11)])
+    LGD_B3G(v[2], v[7], v[8], v[13], m[LGD_S(R, 12)], m[LGD_S(R, 13)])
+    LGD_B3G(v[3], v[4], v[9], v[14], m[LGD_S(R, 14)], m[LGD_S(R, 15)])
+}
+
+// cv <- first 8 words of compress(cv, m, counter = 0, blen, flags)
+__device__ __forceinline__ void b3_compress(uint32_t (&cv)[8], const uint32_t (&m)[16], uint32_t blen,
+                                            uint32_t flags) {
+    uint32_t v[16] = {cv[0], cv[1], cv[2], cv[3], cv[4], cv[5], cv[6], cv[7],
+                      0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au, 0u, 0u, blen, flags};
+    b3_round<0>(v, m);
+    b3_round<1>(v, m);
+    b3_round<2>(v, m);
+    b3_round<3>(v, m);
+    b3_round<4>(v, m);
+    b3_round<5>(v, m);
+    b3_round<6>(v, m);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) cv[i] = v[i] ^ v[i + 8];
+}
+
+__device__ __forceinline__ void b3_iv(uint32_t (&cv)[8]) {
+    cv[0] = 0x6A09E667u; cv[1] = 0xBB67AE85u; cv[2] = 0x3C6EF372u; cv[3] = 0xA54FF53Au;
+    cv[4] = 0x510E527Fu; cv[5] = 0x9B05688Cu; cv[6] = 0x1F83D9ABu; cv[7] = 0x5BE0CD19u;
+}
+
+}  // namespace lgd

@@ -1,0 +1,565 @@
+// CUDA kernels of liblgpu (sm_100a).  All arithmetic is exact GF(2^32) /
+// BLAKE3 integer work; there is no floating point and no tensor-core shape.
+#include "lg_device.cuh"
+#include "lg_kernels.h"
+
+#include <algorithm>
+#include <cstdio>
+
+using namespace lgd;
+
+namespace lgk {
+
+// ---------------------------------------------------------------- Launcher
+cudaEvent_t Launcher::get_event() {
+    if (!free_events.empty()) {
+        cudaEvent_t e = free_events.back();
+        free_events.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+void Launcher::begin(const char *, cudaEvent_t *a) {
+    ++launches;
+    if (!timing) return;
+    *a = get_event();
+    cudaEventRecord(*a, stream);
+}
+void Launcher::end(const char *name, cudaEvent_t a) {
+    if (!timing) return;
+    cudaEvent_t b = get_event();
+    cudaEventRecord(b, stream);
+    pending.push_back({name, a, b});
+}
+void Launcher::resolve() {
+    for (auto &p : pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            auto &s = stats[p.name];
+            s.first += 1;
+            s.second += ms;
+        }
+        free_events.push_back(p.a);
+        free_events.push_back(p.b);
+    }
+    pending.clear();
+}
+void Launcher::release() {
+    for (auto &p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    pending.clear();
+    for (auto e : free_events) cudaEventDestroy(e);
+    free_events.clear();
+}
+
+#define LGK_LAUNCH(L, name, ...)                  \
+    do {                                          \
+        cudaEvent_t _ev = nullptr;                \
+        (L).begin(name, &_ev);                    \
+        __VA_ARGS__;                              \
+        (L).end(name, _ev);                       \
+    } while (0)
+
+static inline unsigned ilog2u(uint64_t x) { unsigned r = 0; while (x > 1) { x >>= 1; ++r; } return r; }
+
+// ====================================================== RS scale + spread
+__global__ void k_rs_scale_spread(const uint32_t *__restrict__ poly, const uint32_t *__restrict__ pis,
+                                  uint32_t *__restrict__ E, uint32_t log_m, uint64_t total) {
+    const uint64_t m = 1ull << log_m;
+    for (uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i = idx & (m - 1), j = idx >> log_m;
+        uint32_t v = gf_mul(poly[idx], pis[i]);
+        uint32_t *col = E + (j << (log_m + 2)) + i;
+        col[0] = v;
+        col[m] = v;
+        col[2 * m] = v;
+        col[3 * m] = v;
+    }
+}
+
+cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *pis, uint32_t *E,
+                            uint32_t log_m, uint32_t n) {
+    uint64_t total = (uint64_t)n << log_m;
+    unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
+    LGK_LAUNCH(L, "rs_scale_spread", k_rs_scale_spread<<<blocks, 256, 0, L.stream>>>(poly, pis, E, log_m, total));
+    return cudaGetLastError();
+}
+
+// ================================================================== FFT
+// One launch = K consecutive stages [d0, d0+K) of every vector.  A thread
+// owns one "pencil": the 2^K rows P*2^(L-d0) + t*S + o (t < 2^K) of one
+// vector, held in registers, S = 2^(L-d0-K).  Threads of a block share
+// (q, P), hence every twiddle of the pass: the block builds the 2^K - 1
+// node tables once and all warps read them broadcast.
+struct PassArgs {
+    uint32_t *data;
+    const uint32_t *tw;
+    uint64_t col_stride, q_stride;
+    uint32_t L, d0, log_S, log_nvec_p2, nvec, log_bpg, log_B, root_base;
+    uint32_t vec_ok;  // 16-byte loads/stores allowed when a pencil is contiguous
+};
+
+template <int K, bool INV>
+__global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
+    extern __shared__ uint32_t tabs[];
+    const unsigned bid = blockIdx.x;
+    const unsigned chunk = bid & ((1u << a.log_bpg) - 1);
+    const unsigned rest = bid >> a.log_bpg;
+    const unsigned P = rest & ((1u << a.d0) - 1);
+    const unsigned q = rest >> a.d0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+    // node (s, t') of this pass = heap node ((root << d0) + P) << s | t'
+    const uint64_t hbase = ((uint64_t)(a.root_base + q) << a.d0) + P;
+    for (int slot = warp; slot < (1 << K) - 1; slot += nw) {
+        const int s = 31 - __clz(slot + 1);
+        const uint64_t heap = (hbase << s) + (uint64_t)(slot + 1 - (1 << s));
+        tab_build_warp(tabs + slot * kTabWords, __ldg(a.tw + heap - 1), lane);
+    }
+    __syncthreads();
+
+    const uint64_t g = ((uint64_t)chunk << a.log_B) + threadIdx.x;
+    const uint64_t o = g & ((1ull << a.log_S) - 1);
+    const uint64_t j = g >> a.log_S;
+    if (j >= a.nvec) return;
+    uint32_t *base = a.data + j * a.col_stride + q * a.q_stride + ((uint64_t)P << (a.L - a.d0)) + o;
+    const uint64_t S = 1ull << a.log_S;
+
+    uint32_t v[1 << K];
+    if (K >= 2 && a.log_S == 0 && a.vec_ok) {
+        const uint4 *b4 = reinterpret_cast<const uint4 *>(base);
+#pragma unroll
+        for (int t = 0; t < (1 << K) / 4; ++t) {
+            uint4 x = b4[t];
+            v[4 * t] = x.x; v[4 * t + 1] = x.y; v[4 * t + 2] = x.z; v[4 * t + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < (1 << K); ++t) v[t] = base[t * S];
+    }
+
+    // One flat loop over the K * 2^(K-1) butterflies so that full unrolling
+    // turns every register index into a constant.  Forward: fft_twiddles /
+    // fft_mul (src/binary_fft.rs:143-159, 180-192), stages root-first.
+    // Inverse: ifft_twiddles / ifft_mul (:161-178, 194-206), leaves-first.
+#pragma unroll
+    for (int it = 0; it < K * (1 << (K - 1)); ++it) {
+        const int s = INV ? K - 1 - (it >> (K - 1)) : (it >> (K - 1));
+        const int w = it & ((1 << (K - 1)) - 1);
+        const int lh = K - s - 1;  // log2 of the butterfly half-length
+        const int tp = w >> lh, u = w & ((1 << lh) - 1);
+        const int x = (tp << (lh + 1)) + u, y = x + (1 << lh);
+        const uint32_t *T = tabs + ((1 << s) - 1 + tp) * kTabWords;
+        if (!INV) {
+            v[x] ^= tab_mul(T, v[y]);
+            v[y] ^= v[x];
+        } else {
+            v[y] ^= v[x];
+            v[x] ^= tab_mul(T, v[y]);
+        }
+    }
+
+    if (K >= 2 && a.log_S == 0 && a.vec_ok) {
+        uint4 *b4 = reinterpret_cast<uint4 *>(base);
+#pragma unroll
+        for (int t = 0; t < (1 << K) / 4; ++t) b4[t] = make_uint4(v[4 * t], v[4 * t + 1], v[4 * t + 2], v[4 * t + 3]);
+    } else {
+#pragma unroll
+        for (int t = 0; t < (1 << K); ++t) base[t * S] = v[t];
+    }
+}
+
+template <bool INV>
+static cudaError_t launch_pass(Launcher &L, int K, PassArgs a, unsigned blocks, unsigned threads) {
+    const size_t smem = (size_t)((1 << K) - 1) * kTabWords * sizeof(uint32_t);
+    char nmbuf[48];
+    std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_pass" : "fft_pass", a.L, K, a.nvec);
+    const char *nm = nmbuf;
+    switch (K) {
+#define LGK_CASE(k) \
+    case k: LGK_LAUNCH(L, nm, k_fft_pass<k, INV><<<blocks, threads, smem, L.stream>>>(a)); break;
+        LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
+#undef LGK_CASE
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
+                        uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
+                        uint32_t root_base, bool inverse) {
+    if (log_len == 0 || nvec == 0) return cudaSuccess;
+    // split log_len stages into passes of <= 6, balanced
+    const uint32_t np = (log_len + 5) / 6;
+    std::vector<uint32_t> ks(np, log_len / np);
+    for (uint32_t i = 0; i < log_len % np; ++i) ks[i] += 1;
+    std::vector<uint32_t> d0s(np);
+    for (uint32_t i = 0, d = 0; i < np; ++i) { d0s[i] = d; d += ks[i]; }
+    uint32_t nvec_p2 = 1;
+    while (nvec_p2 < nvec) nvec_p2 <<= 1;
+    for (uint32_t pi = 0; pi < np; ++pi) {
+        const uint32_t p = inverse ? np - 1 - pi : pi;
+        const uint32_t K = ks[p], d0 = d0s[p];
+        PassArgs a;
+        a.data = data; a.tw = tw; a.col_stride = col_stride; a.q_stride = q_stride;
+        a.L = log_len; a.d0 = d0; a.log_S = log_len - d0 - K;
+        a.log_nvec_p2 = ilog2u(nvec_p2); a.nvec = nvec; a.root_base = root_base;
+        a.vec_ok = ((uintptr_t)data % 16 == 0) && (col_stride % 4 == 0) && (q_stride % 4 == 0);
+        const uint64_t G = (uint64_t)nvec_p2 << a.log_S;  // threads per (q, P)
+        const uint32_t B = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>(G, 256));
+        a.log_B = ilog2u(B);
+        a.log_bpg = ilog2u(G / B);
+        const uint64_t blocks = ((uint64_t)Q << d0) << a.log_bpg;
+        if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+        cudaError_t e = inverse ? launch_pass<true>(L, (int)K, a, (unsigned)blocks, B)
+                                : launch_pass<false>(L, (int)K, a, (unsigned)blocks, B);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// =============================================================== Merkle
+// Leaf = the row's n words as LE bytes, one BLAKE3 chunk (n <= 256):
+// blocks of 16 words, CHUNK_START on the first, CHUNK_END|ROOT on the last.
+__global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
+                            uint32_t *__restrict__ out) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const uint32_t nb = (ncols + 15) / 16;
+    uint32_t cv[8];
+    b3_iv(cv);
+    for (uint32_t b = 0; b < nb; ++b) {
+        uint32_t m[16];
+#pragma unroll
+        for (int w = 0; w < 16; ++w) {
+            const uint32_t j = b * 16 + w;
+            m[w] = j < ncols ? __ldg(E + (uint64_t)j * rows + i) : 0u;
+        }
+        const bool last = b + 1 == nb;
+        const uint32_t blen = last ? 4 * ncols - 64 * (nb - 1) : 64;
+        const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
+        b3_compress(cv, m, blen, flags);
+    }
+    uint4 *o = reinterpret_cast<uint4 *>(out + 8 * i);
+    o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+    o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+}
+
+cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out) {
+    const unsigned blocks = (unsigned)((rows + 127) / 128);
+    LGK_LAUNCH(L, "leaf_hash", k_leaf_hash<<<blocks, 128, 0, L.stream>>>(E, rows, ncols, out));
+    return cudaGetLastError();
+}
+
+// Node = blake3(left || right): one 64-byte block, CHUNK_START|CHUNK_END|ROOT
+// (src/merkle_tree.rs:42-51).  A block reduces 2^c consecutive nodes of one
+// layer through c layers in shared memory and writes every layer it makes.
+__device__ __forceinline__ void hash_node(const uint32_t *l, const uint32_t *r, uint32_t *o) {
+    uint32_t m[16];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) { m[w] = l[w]; m[8 + w] = r[w]; }
+    uint32_t cv[8];
+    b3_iv(cv);
+    b3_compress(cv, m, 64, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) o[w] = cv[w];
+}
+
+__global__ void k_merkle_sub(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in, uint32_t c) {
+    extern __shared__ uint32_t sm[];  // 2 * 2^c * 8 words
+    const uint32_t width = 1u << c;
+    uint32_t *cur = sm, *nxt = sm + 8 * width;
+    const uint64_t first = (uint64_t)blockIdx.x * width;
+    const uint32_t *src = tree + 8 * (in_off + first);
+    for (uint32_t w = threadIdx.x; w < 8 * width; w += blockDim.x) cur[w] = src[w];
+    __syncthreads();
+    uint64_t lay_off = in_off, lay_n = n_in;
+    for (uint32_t l = 1; l <= c; ++l) {
+        const uint32_t cnt = width >> l;
+        const uint64_t next_off = lay_off + lay_n, next_n = lay_n / 2;
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            uint32_t h[8];
+            hash_node(cur + 16 * i, cur + 16 * i + 8, h);
+#pragma unroll
+            for (int w = 0; w < 8; ++w) nxt[8 * i + w] = h[w];
+            uint32_t *dst = tree + 8 * (next_off + (first >> l) + i);
+            reinterpret_cast<uint4 *>(dst)[0] = make_uint4(h[0], h[1], h[2], h[3]);
+            reinterpret_cast<uint4 *>(dst)[1] = make_uint4(h[4], h[5], h[6], h[7]);
+        }
+        __syncthreads();
+        uint32_t *t = cur; cur = nxt; nxt = t;
+        lay_off = next_off;
+        lay_n = next_n;
+    }
+}
+
+cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
+    uint64_t off = 0, n = num_leaves;
+    while (n > 1) {
+        const uint32_t c = std::min<uint32_t>(ilog2u(n), 8);
+        const uint32_t width = 1u << c;
+        const unsigned blocks = (unsigned)(n / width);
+        const unsigned threads = std::max<unsigned>(32, std::min<unsigned>(width / 2, 128));
+        const size_t smem = 2ull * width * 8 * sizeof(uint32_t);
+        LGK_LAUNCH(L, "merkle_layers", k_merkle_sub<<<blocks, threads, smem, L.stream>>>(tree, off, n, c));
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        for (uint32_t l = 0; l < c; ++l) { off += n; n /= 2; }
+    }
+    return cudaSuccess;
+}
+
+// ============================================================== gathers
+__global__ void k_gather_rows(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
+                              const uint64_t *__restrict__ q, uint32_t nq, uint32_t *__restrict__ out) {
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nq * ncols) return;
+    const uint32_t k = idx / ncols, j = idx % ncols;
+    out[idx] = E[(uint64_t)j * rows + q[k]];
+}
+cudaError_t gather_rows(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols,
+                        const uint64_t *d_queries, uint32_t nq, uint32_t *out) {
+    const uint32_t total = nq * ncols;
+    LGK_LAUNCH(L, "gather_rows", k_gather_rows<<<(total + 255) / 256, 256, 0, L.stream>>>(E, rows, ncols, d_queries, nq, out));
+    return cudaGetLastError();
+}
+__global__ void k_gather_nodes(const uint32_t *__restrict__ tree, const uint64_t *__restrict__ idx,
+                               uint32_t count, uint32_t *__restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count * 8) return;
+    out[t] = tree[8 * idx[t / 8] + (t % 8)];
+}
+cudaError_t gather_nodes(Launcher &L, const uint32_t *tree, const uint64_t *d_node_index, uint32_t count,
+                         uint32_t *out) {
+    if (count == 0) return cudaSuccess;
+    LGK_LAUNCH(L, "gather_nodes", k_gather_nodes<<<(count * 8 + 255) / 256, 256, 0, L.stream>>>(tree, d_node_index, count, out));
+    return cudaGetLastError();
+}
+
+// ================================================================= folds
+struct Coeffs64 { uint32_t v[64]; };
+
+// partial_eval over k top variables at once: out[i] = sum_j gr[j] in[j*M+i]
+// with gr the Lagrange (eq) basis of the k challenges; one table per gr[j].
+__global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                                                 uint64_t M, uint32_t nj, Coeffs64 gr) {
+    extern __shared__ uint32_t tabs[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t j = warp; j < nj; j += nw) tab_build_warp(tabs + j * kTabWords, gr.v[j], lane);
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t acc = 0;
+        for (uint32_t j = 0; j < nj; ++j) acc ^= tab_mul(tabs + j * kTabWords, __ldg(in + j * M + i));
+        out[i] = acc;
+    }
+}
+
+cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
+                    const uint32_t *gr) {
+    if (k < 1 || k > 6 || k > log_len) return cudaErrorInvalidValue;
+    Coeffs64 c{};
+    const uint32_t nj = 1u << k;
+    for (uint32_t j = 0; j < nj; ++j) c.v[j] = gr[j];
+    const uint64_t M = 1ull << (log_len - k);
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((M + 255) / 256, 148ull * 8));
+    LGK_LAUNCH(L, "fold_eq", k_fold_eq<<<blocks, 256, nj * kTabWords * sizeof(uint32_t), L.stream>>>(in, out, M, nj, c));
+    return cudaGetLastError();
+}
+
+// =============================================================== sumcheck
+__device__ __forceinline__ uint32_t warp_xor(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void block_xor3(uint32_t s0, uint32_t s1, uint32_t s2, uint32_t *acc3) {
+    __shared__ uint32_t red[3];
+    if (threadIdx.x < 3) red[threadIdx.x] = 0;
+    __syncthreads();
+    s0 = warp_xor(s0); s1 = warp_xor(s1); s2 = warp_xor(s2);
+    if ((threadIdx.x & 31) == 0) { atomicXor(&red[0], s0); atomicXor(&red[1], s1); atomicXor(&red[2], s2); }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicXor(acc3 + threadIdx.x, red[threadIdx.x]);
+}
+
+// evals_at_x with x = 3 (src/ligerito.rs:130-141): 3*hi + (1+3)*lo = x*(hi+lo) + hi
+__device__ __forceinline__ uint32_t at3(uint32_t lo, uint32_t hi) { return gf_mulx(hi ^ lo) ^ hi; }
+
+// eval_013_product (src/multilinear_poly.rs:90-131)
+__global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__restrict__ g, uint64_t half,
+                          uint32_t *acc3) {
+    uint32_t s0 = 0, s1 = 0, s2 = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t f0 = f[i], f1 = f[half + i], g0 = g[i], g1 = g[half + i];
+        s0 ^= gf_mul(f0, g0);
+        s1 ^= gf_mul(f1, g1);
+        s2 ^= gf_mul(at3(f0, f1), at3(g0, g1));
+    }
+    block_xor3(s0, s1, s2, acc3);
+}
+cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t log_len, uint32_t *acc3) {
+    const uint64_t half = 1ull << (log_len - 1);
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((half + 255) / 256, 148ull * 4));
+    LGK_LAUNCH(L, "eval013", k_eval013<<<blocks, 256, 0, L.stream>>>(f, g, half, acc3));
+    return cudaGetLastError();
+}
+
+// SumcheckProverInstance::fold (src/ligerito.rs:119-127): partial_eval of f
+// and of the (summed) basis by r, (1+r)a + r b = a + r(a+b), then
+// eval_01x_product on the folded pair.
+__global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__ f, const uint32_t *__restrict__ B,
+                                                    uint64_t quarter, uint32_t r, uint32_t *__restrict__ fo,
+                                                    uint32_t *__restrict__ Bo, uint32_t *acc3) {
+    __shared__ uint32_t T[kTabWords];
+    if (threadIdx.x < 32) tab_build_warp(T, r, threadIdx.x);
+    __syncthreads();
+    uint32_t s0 = 0, s1 = 0, s2 = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < quarter; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a0 = f[i], a1 = f[quarter + i], a2 = f[2 * quarter + i], a3 = f[3 * quarter + i];
+        const uint32_t c0 = B[i], c1 = B[quarter + i], c2 = B[2 * quarter + i], c3 = B[3 * quarter + i];
+        const uint32_t flo = a0 ^ tab_mul(T, a0 ^ a2), fhi = a1 ^ tab_mul(T, a1 ^ a3);
+        const uint32_t blo = c0 ^ tab_mul(T, c0 ^ c2), bhi = c1 ^ tab_mul(T, c1 ^ c3);
+        fo[i] = flo; fo[quarter + i] = fhi;
+        Bo[i] = blo; Bo[quarter + i] = bhi;
+        s0 ^= gf_mul(flo, blo);
+        s1 ^= gf_mul(fhi, bhi);
+        s2 ^= gf_mul(at3(flo, fhi), at3(blo, bhi));
+    }
+    block_xor3(s0, s1, s2, acc3);
+}
+cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32_t log_len, uint32_t r,
+                       uint32_t *fo, uint32_t *Bo, uint32_t *acc3) {
+    if (log_len < 2) return cudaErrorInvalidValue;
+    const uint64_t quarter = 1ull << (log_len - 2);
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((quarter + 255) / 256, 148ull * 4));
+    LGK_LAUNCH(L, "fold_round", k_fold_round<<<blocks, 256, 0, L.stream>>>(f, B, quarter, r, fo, Bo, acc3));
+    return cudaGetLastError();
+}
+
+// glue (src/ligerito.rs:59-67) folded into the running basis sum
+__global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi, uint64_t n, uint32_t beta) {
+    __shared__ uint32_t T[kTabWords];
+    if (threadIdx.x < 32) tab_build_warp(T, beta, threadIdx.x);
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        B[i] ^= tab_mul(T, bi[i]);
+}
+cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta) {
+    const uint64_t n = 1ull << log_len;
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 4));
+    LGK_LAUNCH(L, "axpy", k_axpy<<<blocks, 256, 0, L.stream>>>(B, bi, n, beta));
+    return cudaGetLastError();
+}
+
+// ================================================================ induce
+// basis[t] = sum_k apow[k] prod_{bit i of t} S_k[i]   (t < 2^n)
+//          = sum_k Hi_k[t >> b] * Lo_k[t & (2^b-1)]
+// Lo_k[u] = prod_{i<b, bit i of u} S_k[i];  Hi_k[c] = apow[k] prod_{i<n-b} S_k[b+i]^bit
+// (field products are associative/commutative, so this grouping equals the
+// reference's doubling order exactly).  The main kernel gives each warp one
+// query at a time: the warp builds the table of Hi_k[block] and multiplies
+// the whole Lo_k vector by it.
+InducePlan induce_plan(uint32_t n, uint32_t nq) {
+    InducePlan p;
+    p.b = std::min<uint32_t>(n, 10);
+    const uint64_t blocks_t = 1ull << (n - p.b);
+    uint32_t qs = 1;
+    while (blocks_t * qs < 296 && qs * 16 < nq) qs *= 2;
+    p.qsplit = qs;
+    p.needs_zero = qs > 1;
+    return p;
+}
+
+__global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__restrict__ apow, uint32_t n,
+                              uint32_t b, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi) {
+    const uint32_t k = blockIdx.x;
+    const uint32_t *Sk = S + (uint64_t)k * n;
+    const uint32_t nlo = 1u << b, nhi = 1u << (n - b);
+    for (uint32_t u = threadIdx.x; u < nlo; u += blockDim.x) {
+        uint32_t p = 1;
+        for (uint32_t i = 0; i < b; ++i)
+            if ((u >> i) & 1) p = gf_mul(p, Sk[i]);
+        lo[(uint64_t)k * nlo + u] = p;
+    }
+    for (uint32_t c = threadIdx.x; c < nhi; c += blockDim.x) {
+        uint32_t p = apow[k];
+        for (uint32_t i = 0; i < n - b; ++i)
+            if ((c >> i) & 1) p = gf_mul(p, Sk[b + i]);
+        hi[(uint64_t)k * nhi + c] = p;
+    }
+}
+
+template <int ACC>  // ACC = max(1, 2^b / 32) words per lane
+__global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
+                                                     uint32_t n, uint32_t b, uint32_t nq, uint32_t qs,
+                                                     uint32_t *__restrict__ out, int atomic_out) {
+    __shared__ uint32_t tabs[8][kTabWords];
+    __shared__ uint32_t red[32 * 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t tb = blockIdx.x, nlo = 1u << b, nhi = 1u << (n - b);
+    const uint32_t per = (nq + qs - 1) / qs, k0 = blockIdx.y * per, k1 = min(nq, k0 + per);
+    uint32_t acc[ACC];
+#pragma unroll
+    for (int c = 0; c < ACC; ++c) acc[c] = 0;
+    for (uint32_t k = k0 + warp; k < k1; k += nw) {
+        tab_build_warp(tabs[warp], __ldg(hi + (uint64_t)k * nhi + tb), lane);
+        __syncwarp();
+        const uint32_t *lk = lo + (uint64_t)k * nlo;
+#pragma unroll
+        for (int c = 0; c < ACC; ++c) {
+            const uint32_t u = lane + 32 * c;
+            if (u < nlo) acc[c] ^= tab_mul(tabs[warp], __ldg(lk + u));
+        }
+        __syncwarp();
+    }
+    for (uint32_t w = threadIdx.x; w < nlo; w += blockDim.x) red[w] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < ACC; ++c) {
+        const uint32_t u = lane + 32 * c;
+        if (u < nlo) atomicXor(&red[u], acc[c]);
+    }
+    __syncthreads();
+    uint32_t *dst = out + (uint64_t)tb * nlo;
+    for (uint32_t w = threadIdx.x; w < nlo; w += blockDim.x) {
+        if (atomic_out) atomicXor(dst + w, red[w]);
+        else dst[w] = red[w];
+    }
+}
+
+cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
+                         uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out) {
+    LGK_LAUNCH(L, "induce_prep", k_induce_prep<<<nq, 256, 0, L.stream>>>(d_S, d_apow, n, p.b, d_lo, d_hi));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dim3 grid(1u << (n - p.b), p.qsplit);
+    const int ao = p.qsplit > 1;
+    switch (std::max<uint32_t>(1, (1u << p.b) / 32)) {
+#define LGK_CASE(a) \
+    case a: LGK_LAUNCH(L, "induce_main", k_induce_main<a><<<grid, 256, 0, L.stream>>>(d_lo, d_hi, n, p.b, nq, p.qsplit, out, ao)); break;
+        LGK_CASE(1) LGK_CASE(2) LGK_CASE(4) LGK_CASE(8) LGK_CASE(16) LGK_CASE(32)
+#undef LGK_CASE
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// ============================================================== splitmix
+__global__ void k_splitmix(uint64_t seed, uint32_t *out, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        out[i] = (uint32_t)(z ^ (z >> 31));
+    }
+}
+cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n) {
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 16));
+    LGK_LAUNCH(L, "splitmix", k_splitmix<<<blocks, 256, 0, L.stream>>>(seed, out, n));
+    return cudaGetLastError();
+}
+
+}  // namespace lgk

@@ -1163,6 +1163,12 @@ static int rb_opening(rbuf *r, arena *a, opening_t *o) {
 static __thread lgref_trace g_trace;
 void lgref_last_trace(lgref_trace *out) { *out = g_trace; }
 
+/* Test hook: a dishonest prover for negative tests.  Bit 0 flips s2 of the
+   final sumcheck round before it is recorded and absorbed, so the proof is
+   transcript-consistent and only the verifier's last check fails. */
+static __thread int g_tamper;
+void lgref_set_tamper(int flags) { g_tamper = flags; }
+
 typedef struct {
     uint32_t *flat; /* column-major, n columns x rows */
     uint8_t *tree;
@@ -1342,6 +1348,10 @@ int lgref_prove(const lgref_config *cfg, const uint32_t *poly, size_t len, int n
             uint32_t ri = lgref_fs_get_field32(&fs);
             g_trace.challenges[g_trace.n_challenges++] = ri;
             sc_fold(&sc, ri, s3, nthreads);
+            if ((g_tamper & 1) && i == cfg->recursive_steps - 1 && t == cfg->ks[i] - 1) {
+                s3[2] ^= 1u;
+                sc.tr[3 * (sc.ntr - 1) + 2] ^= 1u;
+            }
             put_le32(qb, s3[0]); put_le32(qb + 4, s3[1]); put_le32(qb + 8, s3[2]);
             lgref_fs_absorb(&fs, qb, 12);
             rsv[t] = ri;

@@ -133,6 +133,9 @@ typedef struct {
     uint32_t n_sums;
 } lgref_trace;
 void lgref_last_trace(lgref_trace *out);
+/* Test hook (negative tests only): bit 0 = flip s2 of the final sumcheck
+   round; applies to later lgref_prove calls on this thread. */
+void lgref_set_tamper(int flags);
 
 /* ---- seeded input generator (ours; the reference draws unseeded) ---- */
 void lgref_splitmix_coeffs(uint64_t seed, uint32_t *out, size_t n);
