@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -39,8 +40,13 @@ struct lg_ctx {
     std::string err;
     std::map<uint32_t, Code> codes;       // by log_m
     std::map<uint32_t, uint32_t *> ffttw;  // by log_n, plain fft twiddles
-    uint8_t *pinned = nullptr;
+    uint8_t *pinned = nullptr;  // staging for small synchronous transfers
     size_t pinned_cap = 0;
+    // per-call bump arenas (reset at the start of each prove / verify)
+    uint8_t *pin_arena = nullptr;
+    size_t pin_cap = 0, pin_used = 0;
+    uint8_t *dev_arena = nullptr;
+    size_t dev_cap = 0, dev_used = 0;
 };
 
 namespace {
@@ -93,7 +99,6 @@ struct DBuf {
     }
     ~DBuf() { reset(); }
     uint32_t *u32() const { return static_cast<uint32_t *>(p); }
-    uint64_t *u64() const { return static_cast<uint64_t *>(p); }
 };
 
 uint8_t *pinned(lg_ctx *c, size_t bytes) {
@@ -109,12 +114,6 @@ uint8_t *pinned(lg_ctx *c, size_t bytes) {
 
 void sync(lg_ctx *c) { CK(c, cudaStreamSynchronize(c->stream)); }
 
-void h2d(lg_ctx *c, void *dst, const void *src, size_t bytes) {
-    uint8_t *p = pinned(c, bytes);
-    std::memcpy(p, src, bytes);
-    CK(c, cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, c->stream));
-    sync(c);  // the staging buffer is reused by the next transfer
-}
 void d2h(lg_ctx *c, void *dst, const void *src, size_t bytes) {
     uint8_t *p = pinned(c, bytes);
     CK(c, cudaMemcpyAsync(p, src, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -148,6 +147,110 @@ const uint32_t *get_fft_tw(lg_ctx *c, uint32_t log_n) {
     return c->ffttw[log_n] = d;
 }
 
+// ------------------------------------------------------------- scratch
+// Per-call scratch: small device buffers come from a bump arena, uploads
+// and downloads go through a pinned bump arena without synchronising, and
+// host-side results of downloads (openings) are materialised by finalizers
+// after the call's last synchronisation.
+struct Scratch {
+    lg_ctx *c;
+    std::vector<DBuf> dev_overflow;
+    std::vector<std::function<void()>> finalizers;
+    explicit Scratch(lg_ctx *ctx) : c(ctx) {
+        constexpr size_t kPin = 8u << 20, kDev = 32u << 20;
+        if (!c->pin_arena) {
+            CK(c, cudaMallocHost((void **)&c->pin_arena, kPin));
+            c->pin_cap = kPin;
+        }
+        if (!c->dev_arena) {
+            CK(c, cudaMalloc((void **)&c->dev_arena, kDev));
+            c->dev_cap = kDev;
+        }
+        c->pin_used = 0;
+        c->dev_used = 0;
+    }
+    // all pending transfers done, then hand the host copies over
+    void finish() {
+        sync(c);
+        for (auto &f : finalizers) f();
+        finalizers.clear();
+        c->pin_used = 0;
+    }
+    uint8_t *pin(size_t bytes) {
+        bytes = (bytes + 63) & ~size_t(63);
+        if (c->pin_used + bytes > c->pin_cap) {
+            finish();  // drains every transfer that uses the arena
+            if (bytes > c->pin_cap) {
+                cudaFreeHost(c->pin_arena);
+                c->pin_arena = nullptr;
+                size_t cap = std::max(bytes, 2 * c->pin_cap);
+                CK(c, cudaMallocHost((void **)&c->pin_arena, cap));
+                c->pin_cap = cap;
+            }
+        }
+        uint8_t *p = c->pin_arena + c->pin_used;
+        c->pin_used += bytes;
+        return p;
+    }
+    void *dev(size_t bytes) {
+        bytes = (bytes + 255) & ~size_t(255);
+        if (c->dev_used + bytes <= c->dev_cap) {
+            void *p = c->dev_arena + c->dev_used;
+            c->dev_used += bytes;
+            return p;
+        }
+        dev_overflow.emplace_back(c, bytes);
+        return dev_overflow.back().p;
+    }
+    template <class T>
+    T *upload(const T *src, size_t count) {  // async through pinned memory
+        const size_t bytes = count * sizeof(T);
+        uint8_t *h = pin(bytes);
+        std::memcpy(h, src, bytes);
+        T *d = static_cast<T *>(dev(bytes));
+        CK(c, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c->stream));
+        return d;
+    }
+    template <class T>
+    const T *download_later(const T *d, size_t count) {  // valid after finish()
+        const size_t bytes = count * sizeof(T);
+        uint8_t *h = pin(bytes);
+        CK(c, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+        return reinterpret_cast<const T *>(h);
+    }
+};
+
+// Host polynomial to the device: pinned memory is copied directly,
+// pageable memory in pipelined 4 MiB chunks through the pinned arena.
+void upload_poly(lg_ctx *c, Scratch &sc, uint32_t *d, const uint32_t *h, uint64_t len) {
+    const size_t bytes = len * 4;
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, h) == cudaSuccess && attr.type == cudaMemoryTypeHost) {
+        CK(c, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c->stream));
+        return;
+    }
+    cudaGetLastError();
+    constexpr size_t kChunk = 4u << 20;
+    uint8_t *slot[2] = {sc.pin(kChunk), sc.pin(kChunk)};
+    cudaEvent_t ev[2];
+    CK(c, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    CK(c, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    bool used[2] = {false, false};
+    for (size_t off = 0, i = 0; off < bytes; off += kChunk, ++i) {
+        const size_t n = std::min(kChunk, bytes - off);
+        const int k = (int)(i & 1);
+        if (used[k]) CK(c, cudaEventSynchronize(ev[k]));
+        std::memcpy(slot[k], reinterpret_cast<const uint8_t *>(h) + off, n);
+        CK(c, cudaMemcpyAsync(reinterpret_cast<uint8_t *>(d) + off, slot[k], n, cudaMemcpyHostToDevice, c->stream));
+        CK(c, cudaEventRecord(ev[k], c->stream));
+        used[k] = true;
+    }
+    CK(c, cudaEventSynchronize(ev[0]));
+    CK(c, cudaEventSynchronize(ev[1]));
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+}
+
 // ------------------------------------------------------------ commitment
 struct Witness {  // RecursiveLigeroWitness, src/data_structures.rs:32-40
     DBuf E;       // column-major encoded matrix, cols x rows
@@ -167,6 +270,7 @@ void commit_into(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, 
     CK(c, lgk::merkle_upper(c->L, tree, rows));
 }
 
+// commitment + its root on the host (the transcript needs it next)
 Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
     Witness w;
     w.rows = 4ull << log_m;
@@ -179,73 +283,65 @@ Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
 }
 
 // extract_row for each query (src/ligero.rs:40-51) + merkle_tree::prove
-void open(lg_ctx *c, const Witness &w, const std::vector<uint64_t> &q, lg::Opening &out,
-          std::vector<uint32_t> &rows_flat) {
+// (src/merkle_tree.rs:98-111): device gathers, host copies materialised
+// into `out` at sc.finish().  Returns the device copy of the opened rows
+// (nq x cols) and of the queries.
+std::pair<const uint32_t *, const uint64_t *> open_rows(lg_ctx *c, Scratch &sc, const Witness &w,
+                                                        const std::vector<uint64_t> &q, lg::Opening *out) {
     std::vector<NodeRef> refs;
     lg::merkle_proof_nodes(q, w.rows, refs);
     const size_t nq = q.size(), nr = refs.size();
     std::vector<uint64_t> idx(nq + nr);
     std::copy(q.begin(), q.end(), idx.begin());
-    std::vector<uint64_t> layer_off(64, 0);
+    uint64_t layer_off[64] = {0};
     for (uint32_t l = 1; l < 64; ++l) layer_off[l] = layer_off[l - 1] + (w.rows >> (l - 1));
     for (size_t i = 0; i < nr; ++i) idx[nq + i] = layer_off[refs[i].layer] + refs[i].index;
-    DBuf d_idx(c, idx.size() * 8);
-    DBuf d_out(c, (nq * w.cols + nr * 8) * 4 + 16);
-    h2d(c, d_idx.p, idx.data(), idx.size() * 8);
-    CK(c, lgk::gather_rows(c->L, w.E.u32(), w.rows, w.cols, d_idx.u64(), (uint32_t)nq, d_out.u32()));
-    CK(c, lgk::gather_nodes(c->L, w.tree.u32(), d_idx.u64() + nq, (uint32_t)nr, d_out.u32() + nq * w.cols));
-    std::vector<uint32_t> host(nq * w.cols + nr * 8);
-    d2h(c, host.data(), d_out.p, host.size() * 4);
-    rows_flat.assign(host.begin(), host.begin() + nq * w.cols);
-    out.rows.resize(nq);
-    for (size_t k = 0; k < nq; ++k) out.rows[k].assign(host.begin() + k * w.cols, host.begin() + (k + 1) * w.cols);
-    out.merkle.resize(nr);
-    for (size_t i = 0; i < nr; ++i) {
-        const uint8_t *b = reinterpret_cast<const uint8_t *>(host.data() + nq * w.cols + 8 * i);
-        out.merkle[i].assign(b, b + 32);
-    }
+    const uint64_t *d_idx = sc.upload(idx.data(), idx.size());
+    uint32_t *d_out = static_cast<uint32_t *>(sc.dev((nq * w.cols + nr * 8) * 4 + 16));
+    CK(c, lgk::gather_rows(c->L, w.E.u32(), w.rows, w.cols, d_idx, (uint32_t)nq, d_out));
+    CK(c, lgk::gather_nodes(c->L, w.tree.u32(), d_idx + nq, (uint32_t)nr, d_out + nq * w.cols));
+    const uint32_t *h = sc.download_later(d_out, nq * w.cols + nr * 8);
+    const uint32_t cols = w.cols;
+    sc.finalizers.push_back([h, nq, nr, cols, out]() {
+        out->rows.resize(nq);
+        for (size_t k = 0; k < nq; ++k) out->rows[k].assign(h + k * cols, h + (k + 1) * cols);
+        out->merkle.resize(nr);
+        for (size_t i = 0; i < nr; ++i) {
+            const uint8_t *b = reinterpret_cast<const uint8_t *>(h + nq * cols + 8 * i);
+            out->merkle[i].assign(b, b + 32);
+        }
+    });
+    return {d_out, d_idx};
 }
 
-// induce_sumcheck_poly_parallel (src/sumcheck_polys.rs:74-160).  The
-// enforced sum (148 dot products of one row each) is host work; the 2^n
-// basis goes to the device.
-uint32_t induce(lg_ctx *c, uint32_t n, const uint32_t *rows, size_t nrows, const uint32_t *vch, uint32_t nch,
-                const std::vector<uint64_t> &q, uint32_t alpha, uint32_t *d_out) {
-    const size_t glen = 1ull << nch;
+// induce_sumcheck_poly_parallel (src/sumcheck_polys.rs:74-160) entirely on
+// the device from device-resident rows (nq x 2^nch) and queries; the
+// enforced sum lands in d_sum (1 word).
+void induce_dev(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *d_rows, uint32_t nq, const uint32_t *vch,
+                uint32_t nch, const uint64_t *d_q, uint32_t alpha, uint32_t *d_out, uint32_t *d_sum) {
     std::vector<uint32_t> gr = lg::lagrange_basis(vch, nch);
-    std::vector<uint32_t> apow(nrows);
-    uint32_t sum = 0;
-    for (size_t k = 0; k < nrows; ++k) {
-        apow[k] = k ? lg::gf_mul(apow[k - 1], alpha) : 1u;
-        uint32_t dot = 0;
-        for (size_t j = 0; j < glen; ++j) dot ^= lg::gf_mul(rows[k * glen + j], gr[j]);
-        sum ^= lg::gf_mul(dot, apow[k]);
-    }
-    // sks_at_x per query (src/binary_fft.rs:276-301): S[0] = x, S[i] = next_s(S[i-1], sks[i-1])
     std::vector<uint32_t> sks = lg::eval_sk_at_vks(1ull << n);
-    std::vector<uint32_t> S(nrows * std::max<uint32_t>(n, 1));
-    for (size_t k = 0; k < nrows; ++k) {
-        uint32_t *s = S.data() + k * n;
-        if (n == 0) continue;
-        s[0] = (uint32_t)q[k];
-        for (uint32_t i = 1; i < n; ++i) s[i] = lg::next_s(s[i - 1], sks[i - 1]);
-    }
-    lgk::InducePlan plan = lgk::induce_plan(n, (uint32_t)nrows);
-    DBuf dlo(c, nrows * (4ull << plan.b)), dhi(c, nrows * (4ull << (n - plan.b)));
-    std::vector<uint32_t> up(S);
-    up.insert(up.end(), apow.begin(), apow.end());
-    DBuf dup(c, up.size() * 4);
-    h2d(c, dup.p, up.data(), up.size() * 4);
+    lgk::InducePlan plan = lgk::induce_plan(n, nq);
+    uint32_t *d_S = static_cast<uint32_t *>(sc.dev(4ull * nq * std::max<uint32_t>(n, 1)));
+    uint32_t *d_apow = static_cast<uint32_t *>(sc.dev(4ull * nq));
+    uint32_t *d_lo = static_cast<uint32_t *>(sc.dev(4ull * nq << plan.b));
+    uint32_t *d_hi = static_cast<uint32_t *>(sc.dev(4ull * nq << (n - plan.b)));
+    CK(c, lgk::induce_setup(c->L, d_rows, 1u << nch, gr.data(), d_q, nq, alpha, n, sks.data(), d_S, d_apow, d_sum));
     if (plan.needs_zero) CK(c, cudaMemsetAsync(d_out, 0, 4ull << n, c->stream));
-    CK(c, lgk::induce_basis(c->L, plan, dup.u32(), dup.u32() + S.size(), n, (uint32_t)nrows, dlo.u32(),
-                            dhi.u32(), d_out));
-    return sum;
+    CK(c, lgk::induce_basis(c->L, plan, d_S, d_apow, n, nq, d_lo, d_hi, d_out));
 }
 
-std::array<uint32_t, 3> read3(lg_ctx *c, const DBuf &acc) {
-    std::array<uint32_t, 3> s;
-    d2h(c, s.data(), acc.p, 12);
-    return s;
+// host rows / queries (verifier, kernel-level API) -> induce_dev
+uint32_t induce_host_rows(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *rows, size_t nrows,
+                          const uint32_t *vch, uint32_t nch, const std::vector<uint64_t> &q, uint32_t alpha,
+                          uint32_t *d_out) {
+    const uint32_t *d_rows = sc.upload(rows, nrows << nch);
+    const uint64_t *d_q = sc.upload(q.data(), q.size());
+    uint32_t *d_sum = static_cast<uint32_t *>(sc.dev(16));
+    induce_dev(c, sc, n, d_rows, (uint32_t)nrows, vch, nch, d_q, alpha, d_out, d_sum);
+    uint32_t sum = 0;
+    d2h(c, &sum, d_sum, 4);
+    return sum;
 }
 
 // partial_eval by any number of challenges, chunks of <= 6 per launch
@@ -271,17 +367,24 @@ void partial_eval_dev(lg_ctx *c, const uint32_t *d_in, uint32_t log_len, const u
     }
 }
 
+void absorb3(lg::Transcript &fs, const uint32_t *s) { fs.absorb_u32s(s, 3); }
 void absorb3(lg::Transcript &fs, const std::array<uint32_t, 3> &s) { fs.absorb_u32s(s.data(), 3); }
 
 // ------------------------------------------------------------------ prover
-// prover (src/prover.rs:15-199)
-void prove_impl(lg_ctx *c, const lg_config &cfg, const uint32_t *d_poly, uint64_t len, lg::Proof &P) {
+// prover (src/prover.rs:15-199).  The transcript runs on the host; it needs
+// each root, each round triple and yr, so those are the only device->host
+// reads inside the proof.  Openings are downloaded asynchronously and
+// materialised at the end.
+void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_poly, uint64_t len, lg::Proof &P) {
     const size_t s = LG_NUM_QUERIES;
     lg::Transcript fs(LG_FS_SEED);
+    uint32_t *acc = static_cast<uint32_t *>(sc.dev(16));  // s0, s1, s2, enforced sum
+    uint32_t hacc[4];
     Witness w0 = commit(c, d_poly, cfg.initial_log_m, 1u << cfg.initial_log_n);  // :32-37
     P.initial_root.assign(w0.root, w0.root + 32);
     fs.absorb(w0.root, 32);  // :48
 
+    P.recursive.reserve(cfg.recursive_steps);  // openings are filled in by pointer later
     std::vector<uint32_t> pe0(cfg.initial_k);
     for (auto &r : pe0) r = fs.get_field();  // :50
     uint32_t fv = cfg.initial_log_m;         // log2 |f|
@@ -295,34 +398,32 @@ void prove_impl(lg_ctx *c, const lg_config &cfg, const uint32_t *d_poly, uint64_
     std::vector<uint64_t> q;
     if (!fs.get_distinct_queries(w0.rows, s, q)) throw ProverAssert{};  // :67
     const uint32_t alpha = fs.get_field();                             // :68
-    std::vector<uint32_t> rows;
-    open(c, w0, q, P.initial, rows);  // :72-76
+    auto opened = open_rows(c, sc, w0, q, &P.initial);                 // :72-76
+    DBuf B(c, 4ull << fv);
+    CK(c, cudaMemsetAsync(acc, 0, 16, c->stream));
+    induce_dev(c, sc, fv, opened.first, (uint32_t)s, pe0.data(), cfg.initial_k, opened.second, alpha, B.u32(),
+               acc + 3);  // :78-85
     w0.E.reset();
     w0.tree.reset();
-    DBuf B(c, 4ull << fv);
-    const uint32_t h1 = induce(c, fv, rows.data(), s, pe0.data(), cfg.initial_k, q, alpha, B.u32());  // :78-85
-
-    DBuf acc(c, 16);
-    CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
-    CK(c, lgk::eval013(c->L, f.u32(), B.u32(), fv, acc.u32()));  // SumcheckProverInstance::new
-    std::array<uint32_t, 3> s3 = read3(c, acc);
-    if ((s3[0] ^ s3[1]) != h1) throw ProverAssert{};  // src/ligerito.rs:35
-    P.transcript.push_back(s3);
-    absorb3(fs, s3);  // :93
+    CK(c, lgk::eval013(c->L, f.u32(), B.u32(), fv, acc));  // SumcheckProverInstance::new
+    d2h(c, hacc, acc, 16);
+    if ((hacc[0] ^ hacc[1]) != hacc[3]) throw ProverAssert{};  // src/ligerito.rs:35
+    P.transcript.push_back({hacc[0], hacc[1], hacc[2]});
+    absorb3(fs, hacc);  // :93
 
     DBuf f2(c, 4ull << (fv - 1)), B2(c, 4ull << (fv - 1));
     for (uint32_t i = 0; i < cfg.recursive_steps; ++i) {
         std::vector<uint32_t> rs;
         for (uint32_t t = 0; t < cfg.ks[i]; ++t) {  // :97-102
             const uint32_t r = fs.get_field();
-            CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
-            CK(c, lgk::fold_round(c->L, f.u32(), B.u32(), fv, r, f2.u32(), B2.u32(), acc.u32()));
+            CK(c, cudaMemsetAsync(acc, 0, 12, c->stream));
+            CK(c, lgk::fold_round(c->L, f.u32(), B.u32(), fv, r, f2.u32(), B2.u32(), acc));
             std::swap(f, f2);
             std::swap(B, B2);
             fv -= 1;
-            s3 = read3(c, acc);
-            P.transcript.push_back(s3);
-            absorb3(fs, s3);
+            d2h(c, hacc, acc, 12);
+            P.transcript.push_back({hacc[0], hacc[1], hacc[2]});
+            absorb3(fs, hacc);
             rs.push_back(r);
         }
         if (i == cfg.recursive_steps - 1) {  // :104-143
@@ -330,7 +431,7 @@ void prove_impl(lg_ctx *c, const lg_config &cfg, const uint32_t *d_poly, uint64_
             d2h(c, P.yr.data(), f.p, 4ull << fv);
             fs.absorb_u32s(P.yr.data(), P.yr.size());
             if (!fs.get_distinct_queries(wprev.rows, s, q)) throw ProverAssert{};
-            open(c, wprev, q, P.final_, rows);
+            open_rows(c, sc, wprev, q, &P.final_);
             return;
         }
         Witness wn = commit(c, f.u32(), cfg.log_m[i + 1], 1u << cfg.log_n[i + 1]);  // :145-155
@@ -338,17 +439,16 @@ void prove_impl(lg_ctx *c, const lg_config &cfg, const uint32_t *d_poly, uint64_
         P.recursive_roots.push_back(std::vector<uint8_t>(wn.root, wn.root + 32));
         if (!fs.get_distinct_queries(wprev.rows, s, q)) throw ProverAssert{};  // :157
         const uint32_t al = fs.get_field();                                  // :158
-        lg::Opening op;
-        open(c, wprev, q, op, rows);  // :161-172
-        P.recursive.push_back(std::move(op));
+        P.recursive.emplace_back();
+        auto op = open_rows(c, sc, wprev, q, &P.recursive.back());  // :161-172
         DBuf bi(c, 4ull << fv);
-        const uint32_t h = induce(c, fv, rows.data(), s, rs.data(), cfg.ks[i], q, al, bi.u32());  // :174-181
-        CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
-        CK(c, lgk::eval013(c->L, f.u32(), bi.u32(), fv, acc.u32()));  // introduce_new
-        s3 = read3(c, acc);
-        if ((s3[0] ^ s3[1]) != h) throw ProverAssert{};  // src/ligerito.rs:52
-        P.transcript.push_back(s3);
-        absorb3(fs, s3);  // :187-191
+        CK(c, cudaMemsetAsync(acc, 0, 16, c->stream));
+        induce_dev(c, sc, fv, op.first, (uint32_t)s, rs.data(), cfg.ks[i], op.second, al, bi.u32(), acc + 3);
+        CK(c, lgk::eval013(c->L, f.u32(), bi.u32(), fv, acc));  // introduce_new
+        d2h(c, hacc, acc, 16);
+        if ((hacc[0] ^ hacc[1]) != hacc[3]) throw ProverAssert{};  // src/ligerito.rs:52
+        P.transcript.push_back({hacc[0], hacc[1], hacc[2]});
+        absorb3(fs, hacc);  // :187-191
         const uint32_t beta = fs.get_field();  // :193
         CK(c, lgk::axpy(c->L, B.u32(), bi.u32(), fv, beta));  // glue
         wprev = std::move(wn);
@@ -425,7 +525,7 @@ void ligero_verify_host(const std::vector<uint64_t> &q, const lg::Opening &o, co
     }
 }
 
-bool verify_impl(lg_ctx *c, const lg_config &cfg, const lg::Proof &P) {
+bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &P) {
     const size_t s = LG_NUM_QUERIES;
     const uint32_t log_inv_rate = 2;  // src/verifier.rs:26
     lg::Transcript fs(LG_FS_SEED);
@@ -445,8 +545,8 @@ bool verify_impl(lg_ctx *c, const lg_config &cfg, const lg::Proof &P) {
     basis.emplace_back(c, 4ull << cfg.initial_log_m);
     bvars.push_back(cfg.initial_log_m);
     sep.push_back(1);
-    const uint32_t h1 = induce(c, cfg.initial_log_m, rows.data(), s, pe0.data(), cfg.initial_k, q, alpha,
-                               basis.back().u32());  // :53-60
+    const uint32_t h1 = induce_host_rows(c, sc, cfg.initial_log_m, rows.data(), s, pe0.data(), cfg.initial_k, q,
+                                         alpha, basis.back().u32());  // :53-60
     // SumcheckVerifierInstance::new (src/ligerito.rs:172-192)
     size_t rd = 0;
     auto read_tr = [&]() {
@@ -519,7 +619,8 @@ bool verify_impl(lg_ctx *c, const lg_config &cfg, const lg::Proof &P) {
         std::vector<uint32_t> rr = dense(P.recursive[i], s, 1ull << cfg.ks[i]);
         basis.emplace_back(c, 4ull << cfg.log_m[i]);
         bvars.push_back(cfg.log_m[i]);
-        const uint32_t h = induce(c, cfg.log_m[i], rr.data(), s, rs.data(), cfg.ks[i], q, al, basis.back().u32());
+        const uint32_t h = induce_host_rows(c, sc, cfg.log_m[i], rr.data(), s, rs.data(), cfg.ks[i], q, al,
+                                            basis.back().u32());
         g = read_tr();  // introduce_new (src/ligerito.rs:212-220)
         if ((g[0] ^ g[1]) != h) throw VerifyPanic{};
         Quad to_glue = quad_from_evals(g[0], g[1], g[2]);
@@ -656,6 +757,8 @@ void lg_ctx_destroy(lg_ctx *c) {
     for (auto &kv : c->codes) { cudaFree(kv.second.tw); cudaFree(kv.second.pis); }
     for (auto &kv : c->ffttw) cudaFree(kv.second);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->pin_arena) cudaFreeHost(c->pin_arena);
+    if (c->dev_arena) cudaFree(c->dev_arena);
     c->L.release();
     cudaStreamDestroy(c->stream);
     delete c;
@@ -703,14 +806,15 @@ lg_status lg_prove(lg_ctx *c, const lg_config *cfg, const uint32_t *poly, uint64
     if (!res) return LG_ERR_OUT_OF_MEMORY;
     st = guarded(c, [&] {
         CK(c, cudaSetDevice(c->device));
+        Scratch sc(c);
         if (on_device) {
-            prove_impl(c, *cfg, poly, len, res->p);
+            prove_impl(c, sc, *cfg, poly, len, res->p);
         } else {
             DBuf d(c, len * 4);
-            CK(c, cudaMemcpyAsync(d.p, poly, len * 4, cudaMemcpyHostToDevice, c->stream));
-            prove_impl(c, *cfg, d.u32(), len, res->p);
+            upload_poly(c, sc, d.u32(), poly, len);
+            prove_impl(c, sc, *cfg, d.u32(), len, res->p);
         }
-        sync(c);
+        sc.finish();
     });
     if (st != LG_OK) { delete res; return st; }
     *out = res;
@@ -728,8 +832,9 @@ lg_status lg_verify(lg_ctx *c, const lg_config *cfg, const lg_proof *proof, int 
     bool ok = false;
     lg_status st = guarded(c, [&] {
         CK(c, cudaSetDevice(c->device));
-        ok = verify_impl(c, *cfg, proof->p);
-        sync(c);
+        Scratch sc(c);
+        ok = verify_impl(c, sc, *cfg, proof->p);
+        sc.finish();
     });
     if (st == LG_OK) *accepted = ok ? 1 : 0;
     return st;
@@ -822,8 +927,7 @@ lg_status lg_eval_013_product(lg_ctx *c, const uint32_t *d_f, const uint32_t *d_
         DBuf acc(c, 16);
         CK(c, cudaMemsetAsync(acc.p, 0, 12, c->stream));
         CK(c, lgk::eval013(c->L, d_f, d_g, log_len, acc.u32()));
-        std::array<uint32_t, 3> s = read3(c, acc);
-        out[0] = s[0]; out[1] = s[1]; out[2] = s[2];
+        d2h(c, out, acc.p, 12);
     });
 }
 
@@ -837,8 +941,9 @@ lg_status lg_induce_sumcheck_poly(lg_ctx *c, uint32_t n, const uint32_t *rows, u
     return guarded(c, [&] {
         CK(c, cudaSetDevice(c->device));
         std::vector<uint64_t> q(queries, queries + nrows);
-        *enforced_sum = induce(c, n, rows, nrows, vch, nch, q, alpha, d_out);
-        sync(c);
+        Scratch sc(c);
+        *enforced_sum = induce_host_rows(c, sc, n, rows, nrows, vch, nch, q, alpha, d_out);
+        sc.finish();
     });
 }
 

@@ -72,13 +72,27 @@ __device__ __forceinline__ void tab_build_warp(uint32_t *T, uint32_t c, int lane
     T[96 + lane] = v;
 }
 
-// c * w, with T the table of c
-__device__ __forceinline__ uint32_t tab_mul(const uint32_t *__restrict__ T, uint32_t w) {
-    uint32_t r0 = T[w & 15u] ^ T[16 + ((w >> 4) & 15u)];
-    uint32_t r1 = T[32 + ((w >> 8) & 15u)] ^ T[48 + ((w >> 12) & 15u)];
-    uint32_t r2 = T[64 + ((w >> 16) & 15u)] ^ T[80 + ((w >> 20) & 15u)];
-    uint32_t r3 = T[96 + ((w >> 24) & 15u)] ^ T[112 + (w >> 28)];
-    return (r0 ^ r1) ^ (r2 ^ r3);
+// Same product with the table at byte offset base + off of the shared
+// array `sm`, base a multiple of 256 (its low byte is zero) and off a
+// constant after unrolling.  Byte j of a (b) holds 4 * nibble 2j (2j+1) of
+// w, the byte offset of that window's entry; one byte-permute splices it
+// under `base`, and off + the window's 64-byte slot fold into the load's
+// immediate.  Per product: 4 ops to spread the nibbles, 8 permutes, 8
+// loads, 4 XORs.
+__device__ __forceinline__ uint32_t shared_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint32_t tab_mul_sa(const uint8_t *__restrict__ sm, uint32_t base, uint32_t off,
+                                               uint32_t w) {
+    const uint32_t a = (w << 2) & 0x3C3C3C3Cu;
+    const uint32_t b = (w >> 2) & 0x3C3C3C3Cu;
+#define LGD_LD(x, sel, o) (*reinterpret_cast<const uint32_t *>(sm + __byte_perm((x), base, (sel)) + off + (o)))
+    const uint32_t r0 = LGD_LD(a, 0x7650, 0), r1 = LGD_LD(b, 0x7650, 64);
+    const uint32_t r2 = LGD_LD(a, 0x7651, 128), r3 = LGD_LD(b, 0x7651, 192);
+    const uint32_t r4 = LGD_LD(a, 0x7652, 256), r5 = LGD_LD(b, 0x7652, 320);
+    const uint32_t r6 = LGD_LD(a, 0x7653, 384), r7 = LGD_LD(b, 0x7653, 448);
+#undef LGD_LD
+    return (r0 ^ r1 ^ r2) ^ (r3 ^ r4 ^ r5) ^ (r6 ^ r7);
 }
 
 // ---------------------------------------------------------------- BLAKE3

@@ -94,6 +94,54 @@ static void sha256_compress(uint32_t st[8], const uint8_t blk[64]) {
     st[0] += a; st[1] += b; st[2] += c; st[3] += d; st[4] += e; st[5] += f; st[6] += g; st[7] += h;
 }
 
+#if defined(__x86_64__)
+// The same compression with the x86 SHA extensions.  The state is kept as
+// (A,B,E,F) / (C,D,G,H) halves as sha256rnds2 expects; each 4-round group
+// adds the schedule words and round constants, and words 16..63 come from
+// sha256msg1 / sha256msg2: W[t..t+3] = msg2(msg1(W[t-16..], W[t-12..]) +
+// W[t-7..t-4], W[t-4..t-1]).
+__attribute__((target("sha,sse4.1,ssse3"))) static void sha256_compress_ni(uint32_t st[8], const uint8_t blk[64]) {
+    const __m128i bswap = _mm_set_epi64x(0x0c0d0e0f08090a0bULL, 0x0405060700010203ULL);
+    __m128i dcba = _mm_loadu_si128(reinterpret_cast<const __m128i *>(st));
+    __m128i hgfe = _mm_loadu_si128(reinterpret_cast<const __m128i *>(st + 4));
+    __m128i cdab = _mm_shuffle_epi32(dcba, 0xB1);
+    __m128i efgh = _mm_shuffle_epi32(hgfe, 0x1B);
+    __m128i abef = _mm_alignr_epi8(cdab, efgh, 8);
+    __m128i cdgh = _mm_blend_epi16(efgh, cdab, 0xF0);
+    const __m128i abef0 = abef, cdgh0 = cdgh;
+    __m128i m[4];
+    for (int i = 0; i < 4; ++i)
+        m[i] = _mm_shuffle_epi8(_mm_loadu_si128(reinterpret_cast<const __m128i *>(blk + 16 * i)), bswap);
+    for (int i = 0; i < 16; ++i) {
+        __m128i w;
+        if (i < 4) {
+            w = m[i];
+        } else {
+            __m128i x = _mm_sha256msg1_epu32(m[i & 3], m[(i + 1) & 3]);
+            x = _mm_add_epi32(x, _mm_alignr_epi8(m[(i + 3) & 3], m[(i + 2) & 3], 4));
+            w = m[i & 3] = _mm_sha256msg2_epu32(x, m[(i + 3) & 3]);
+        }
+        __m128i k = _mm_add_epi32(w, _mm_loadu_si128(reinterpret_cast<const __m128i *>(K256 + 4 * i)));
+        cdgh = _mm_sha256rnds2_epu32(cdgh, abef, k);
+        abef = _mm_sha256rnds2_epu32(abef, cdgh, _mm_shuffle_epi32(k, 0x0E));
+    }
+    abef = _mm_add_epi32(abef, abef0);
+    cdgh = _mm_add_epi32(cdgh, cdgh0);
+    __m128i feba = _mm_shuffle_epi32(abef, 0x1B);
+    __m128i dchg = _mm_shuffle_epi32(cdgh, 0xB1);
+    _mm_storeu_si128(reinterpret_cast<__m128i *>(st), _mm_blend_epi16(feba, dchg, 0xF0));
+    _mm_storeu_si128(reinterpret_cast<__m128i *>(st + 4), _mm_alignr_epi8(dchg, feba, 8));
+}
+static const bool g_has_shani = __builtin_cpu_supports("sha") && __builtin_cpu_supports("sse4.1");
+#endif
+
+static void sha256_block(uint32_t st[8], const uint8_t blk[64]) {
+#if defined(__x86_64__)
+    if (g_has_shani) { sha256_compress_ni(st, blk); return; }
+#endif
+    sha256_compress(st, blk);
+}
+
 Sha256::Sha256() {
     static const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
                                    0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
@@ -106,9 +154,9 @@ void Sha256::update(const uint8_t *p, size_t len) {
         size_t take = std::min(len, 64 - n);
         std::memcpy(buf + n, p, take);
         n += take; p += take; len -= take;
-        if (n == 64) { sha256_compress(h, buf); n = 0; }
+        if (n == 64) { sha256_block(h, buf); n = 0; }
     }
-    while (len >= 64) { sha256_compress(h, p); p += 64; len -= 64; }
+    while (len >= 64) { sha256_block(h, p); p += 64; len -= 64; }
     if (len) { std::memcpy(buf, p, len); n = len; }
 }
 
@@ -121,8 +169,8 @@ void Sha256::finish(uint8_t out[32]) const {
     size_t tl = (n + 1 + 8 <= 64) ? 64 : 128;
     uint64_t bits = total * 8;
     for (int i = 0; i < 8; ++i) tail[tl - 1 - i] = (uint8_t)(bits >> (8 * i));
-    sha256_compress(st, tail);
-    if (tl == 128) sha256_compress(st, tail + 64);
+    sha256_block(st, tail);
+    if (tl == 128) sha256_block(st, tail + 64);
     for (int i = 0; i < 8; ++i) {
         out[4 * i] = (uint8_t)(st[i] >> 24); out[4 * i + 1] = (uint8_t)(st[i] >> 16);
         out[4 * i + 2] = (uint8_t)(st[i] >> 8); out[4 * i + 3] = (uint8_t)st[i];

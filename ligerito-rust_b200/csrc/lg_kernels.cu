@@ -88,36 +88,79 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
 }
 
 // ================================================================== FFT
-// One launch = K consecutive stages [d0, d0+K) of every vector.  A thread
-// owns one "pencil": the 2^K rows P*2^(L-d0) + t*S + o (t < 2^K) of one
-// vector, held in registers, S = 2^(L-d0-K).  Threads of a block share
-// (q, P), hence every twiddle of the pass: the block builds the 2^K - 1
-// node tables once and all warps read them broadcast.
+// A launch runs K consecutive stages [d0, d0+K) of every vector.  Vector
+// (j, q) starts at data + j*col_stride + q*q_stride and uses the twiddle
+// subtree under heap node root_base + q; the node of stage d0+s with
+// in-pass index t' is heap node ((root << d0) + P) << s | t'.
 struct PassArgs {
     uint32_t *data;
     const uint32_t *tw;
     uint64_t col_stride, q_stride;
     uint32_t L, d0, log_S, log_nvec_p2, nvec, log_bpg, log_B, root_base;
-    uint32_t vec_ok;  // 16-byte loads/stores allowed when a pencil is contiguous
+    uint32_t vec_ok;            // 16-byte loads/stores allowed when a pencil is contiguous
+    uint32_t vchunk, nchunks;   // tail kernel: vectors per block, blocks per (q, P)
 };
 
+// Builds the 2^K - 1 node tables of one (q, P) in 512-byte slots at the
+// start of `sm` (tab_mul_sa needs table offsets that are multiples of 256
+// relative to the array); returns the offset of slot 0.
+template <int K>
+__device__ __forceinline__ uint32_t build_pass_tables(uint8_t *sm, const PassArgs &a, unsigned q, unsigned P) {
+    const uint32_t toff = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint64_t hbase = ((uint64_t)(a.root_base + q) << a.d0) + P;
+    for (int slot = warp; slot < (1 << K) - 1; slot += nw) {
+        const int s = 31 - __clz(slot + 1);
+        const uint64_t heap = (hbase << s) + (uint64_t)(slot + 1 - (1 << s));
+        tab_build_warp(reinterpret_cast<uint32_t *>(sm + toff + slot * 512), __ldg(a.tw + heap - 1), lane);
+    }
+    return toff;
+}
+
+// K stages over the NV values of a register pencil, node index of value i at
+// in-pass stage s = (i >> (K - s)) + node_off(s); tables at tb + 512 * slot.
+// Forward: fft_twiddles / fft_mul (src/binary_fft.rs:143-159, 180-192),
+// stages root-first.  Inverse: ifft_twiddles / ifft_mul (:161-178,
+// 194-206), leaves-first.  One flat loop so every register index is a
+// compile-time constant after unrolling.
+template <int KP, int S0, bool INV>
+__device__ __forceinline__ void pencil_stages(uint32_t (&v)[1 << KP], const uint8_t *sm, uint32_t tb,
+                                              uint32_t gshift_slot) {
+#pragma unroll
+    for (int it = 0; it < KP * (1 << (KP - 1)); ++it) {
+        const int sl = INV ? KP - 1 - (it >> (KP - 1)) : (it >> (KP - 1));  // stage within the phase
+        const int s = S0 + sl;                                                  // stage within the pass
+        const int w = it & ((1 << (KP - 1)) - 1);
+        const int lh = KP - sl - 1;
+        const int tp = w >> lh, u = w & ((1 << lh) - 1);
+        const int x = (tp << (lh + 1)) + u, y = x + (1 << lh);
+        // gshift_slot: runtime prefix of the node index inside this stage,
+        // folded into the (256-aligned) base; the rest is a constant offset
+        const uint32_t base = tb + 512u * (gshift_slot << sl);
+        const uint32_t off = 512u * ((1u << s) - 1u + (uint32_t)tp);
+        if (!INV) {
+            v[x] ^= tab_mul_sa(sm, base, off, v[y]);
+            v[y] ^= v[x];
+        } else {
+            v[y] ^= v[x];
+            v[x] ^= tab_mul_sa(sm, base, off, v[y]);
+        }
+    }
+}
+
+// Strided passes: a thread owns one "pencil", the 2^K rows
+// P*2^(L-d0) + t*S + o (t < 2^K) of one vector, S = 2^(L-d0-K) > 1, in
+// registers.  Threads of a block share (q, P) and hence every twiddle of
+// the pass; lanes run over o, so each row access is coalesced.
 template <int K, bool INV>
 __global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
-    extern __shared__ uint32_t tabs[];
+    extern __shared__ __align__(16) uint8_t smraw[];
     const unsigned bid = blockIdx.x;
     const unsigned chunk = bid & ((1u << a.log_bpg) - 1);
     const unsigned rest = bid >> a.log_bpg;
     const unsigned P = rest & ((1u << a.d0) - 1);
     const unsigned q = rest >> a.d0;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
-    // node (s, t') of this pass = heap node ((root << d0) + P) << s | t'
-    const uint64_t hbase = ((uint64_t)(a.root_base + q) << a.d0) + P;
-    for (int slot = warp; slot < (1 << K) - 1; slot += nw) {
-        const int s = 31 - __clz(slot + 1);
-        const uint64_t heap = (hbase << s) + (uint64_t)(slot + 1 - (1 << s));
-        tab_build_warp(tabs + slot * kTabWords, __ldg(a.tw + heap - 1), lane);
-    }
+    const uint32_t tb = build_pass_tables<K>(smraw, a, q, P);
     __syncthreads();
 
     const uint64_t g = ((uint64_t)chunk << a.log_B) + threadIdx.x;
@@ -126,61 +169,123 @@ __global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
     if (j >= a.nvec) return;
     uint32_t *base = a.data + j * a.col_stride + q * a.q_stride + ((uint64_t)P << (a.L - a.d0)) + o;
     const uint64_t S = 1ull << a.log_S;
-
     uint32_t v[1 << K];
-    if (K >= 2 && a.log_S == 0 && a.vec_ok) {
-        const uint4 *b4 = reinterpret_cast<const uint4 *>(base);
 #pragma unroll
-        for (int t = 0; t < (1 << K) / 4; ++t) {
-            uint4 x = b4[t];
-            v[4 * t] = x.x; v[4 * t + 1] = x.y; v[4 * t + 2] = x.z; v[4 * t + 3] = x.w;
-        }
-    } else {
+    for (int t = 0; t < (1 << K); ++t) v[t] = base[t * S];
+    pencil_stages<K, 0, INV>(v, smraw, tb, 0);
+    // recompute the store addresses instead of keeping 2^K pointers live
+    uint64_t S2;
+    asm volatile("mov.b64 %0, %1;" : "=l"(S2) : "l"(S));
+    uint32_t *base2;
+    asm volatile("mov.b64 %0, %1;" : "=l"(base2) : "l"(base));
 #pragma unroll
-        for (int t = 0; t < (1 << K); ++t) v[t] = base[t * S];
-    }
+    for (int t = 0; t < (1 << K); ++t) base2[t * S2] = v[t];
+}
 
-    // One flat loop over the K * 2^(K-1) butterflies so that full unrolling
-    // turns every register index into a constant.  Forward: fft_twiddles /
-    // fft_mul (src/binary_fft.rs:143-159, 180-192), stages root-first.
-    // Inverse: ifft_twiddles / ifft_mul (:161-178, 194-206), leaves-first.
-#pragma unroll
-    for (int it = 0; it < K * (1 << (K - 1)); ++it) {
-        const int s = INV ? K - 1 - (it >> (K - 1)) : (it >> (K - 1));
-        const int w = it & ((1 << (K - 1)) - 1);
-        const int lh = K - s - 1;  // log2 of the butterfly half-length
-        const int tp = w >> lh, u = w & ((1 << lh) - 1);
-        const int x = (tp << (lh + 1)) + u, y = x + (1 << lh);
-        const uint32_t *T = tabs + ((1 << s) - 1 + tp) * kTabWords;
-        if (!INV) {
-            v[x] ^= tab_mul(T, v[y]);
-            v[y] ^= v[x];
-        } else {
-            v[y] ^= v[x];
-            v[x] ^= tab_mul(T, v[y]);
-        }
-    }
+// Last pass (contiguous blocks of 2^K rows): one block per (q, P) tile of
+// 2^K rows x nvec vectors.  The tile is loaded with coalesced 16-byte reads
+// into shared memory with an odd column stride (2^K + 1 words), so both a
+// lane-per-vector walk down a column and a lane-per-row walk across the
+// columns are bank-conflict free.  All warps build the 2^K - 1 tables, then
+// the stages run in two register phases: KA = K-4 stages on 2^KA-value
+// pencils (rows u + 16i), then 4 stages on 16 contiguous rows.  Lanes run
+// over vectors, so a warp shares every table it reads.
+template <int K, bool INV>
+__global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
+    constexpr int KA = K - 4, R = 1 << K, STRIDE = R + 1, CPC = R / 4;
+    extern __shared__ __align__(16) uint8_t smraw[];
+    const unsigned chunk = blockIdx.x % a.nchunks, rest = blockIdx.x / a.nchunks;
+    const unsigned P = rest & ((1u << a.d0) - 1);
+    const unsigned q = rest >> a.d0;
+    const uint32_t nvec = min(a.vchunk, a.nvec - chunk * a.vchunk);
+    const uint32_t tb = build_pass_tables<K>(smraw, a, q, P);
+    uint32_t *tile = reinterpret_cast<uint32_t *>(smraw + tb + ((1 << K) - 1) * 512);
+    uint32_t *gbase = a.data + (uint64_t)chunk * a.vchunk * a.col_stride + q * a.q_stride + ((uint64_t)P << K);
 
-    if (K >= 2 && a.log_S == 0 && a.vec_ok) {
-        uint4 *b4 = reinterpret_cast<uint4 *>(base);
+    for (uint32_t c = threadIdx.x; c < nvec * CPC; c += blockDim.x) {
+        const uint32_t j = c / CPC, piece = c % CPC;
+        const uint4 x = *reinterpret_cast<const uint4 *>(gbase + j * a.col_stride + 4 * piece);
+        uint32_t *d = tile + j * STRIDE + 4 * piece;
+        d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w;
+    }
+    __syncthreads();
+
+    auto phase_a = [&]() {
+        if constexpr (KA > 0) {
+            for (uint32_t item = threadIdx.x; item < nvec * 16; item += blockDim.x) {
+                const uint32_t j = item % nvec, u = item / nvec;
+                uint32_t v[1 << KA];
 #pragma unroll
-        for (int t = 0; t < (1 << K) / 4; ++t) b4[t] = make_uint4(v[4 * t], v[4 * t + 1], v[4 * t + 2], v[4 * t + 3]);
+                for (int i = 0; i < (1 << KA); ++i) v[i] = tile[j * STRIDE + u + 16 * i];
+                pencil_stages<KA, 0, INV>(v, smraw, tb, 0);
+#pragma unroll
+                for (int i = 0; i < (1 << KA); ++i) tile[j * STRIDE + u + 16 * i] = v[i];
+            }
+        }
+    };
+    auto phase_b = [&]() {
+        for (uint32_t item = threadIdx.x; item < (nvec << KA); item += blockDim.x) {
+            const uint32_t j = item % nvec, gq = item / nvec;
+            uint32_t v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = tile[j * STRIDE + 16 * gq + i];
+            pencil_stages<4, KA, INV>(v, smraw, tb, gq);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) tile[j * STRIDE + 16 * gq + i] = v[i];
+        }
+    };
+    if (!INV) {
+        phase_a();
+        __syncthreads();
+        phase_b();
     } else {
-#pragma unroll
-        for (int t = 0; t < (1 << K); ++t) base[t * S] = v[t];
+        phase_b();
+        __syncthreads();
+        phase_a();
+    }
+    __syncthreads();
+
+    for (uint32_t c = threadIdx.x; c < nvec * CPC; c += blockDim.x) {
+        const uint32_t j = c / CPC, piece = c % CPC;
+        const uint32_t *d = tile + j * STRIDE + 4 * piece;
+        *reinterpret_cast<uint4 *>(gbase + j * a.col_stride + 4 * piece) = make_uint4(d[0], d[1], d[2], d[3]);
     }
 }
 
+static size_t pass_smem(int K) { return (size_t)((1 << K) - 1) * 512; }
+static size_t tail_smem(int K, uint32_t nvec) { return pass_smem(K) + (size_t)nvec * ((1u << K) + 1) * 4; }
+
 template <bool INV>
 static cudaError_t launch_pass(Launcher &L, int K, PassArgs a, unsigned blocks, unsigned threads) {
-    const size_t smem = (size_t)((1 << K) - 1) * kTabWords * sizeof(uint32_t);
     char nmbuf[48];
     std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_pass" : "fft_pass", a.L, K, a.nvec);
-    const char *nm = nmbuf;
+    const size_t smem = pass_smem(K);
     switch (K) {
-#define LGK_CASE(k) \
-    case k: LGK_LAUNCH(L, nm, k_fft_pass<k, INV><<<blocks, threads, smem, L.stream>>>(a)); break;
+#define LGK_CASE(k)                                                                                  \
+    case k:                                                                                          \
+        if (smem > 48 * 1024)                                                                        \
+            cudaFuncSetAttribute(k_fft_pass<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        LGK_LAUNCH(L, nmbuf, k_fft_pass<k, INV><<<blocks, threads, smem, L.stream>>>(a));            \
+        break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
+#undef LGK_CASE
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <bool INV>
+static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) {
+    char nmbuf[48];
+    std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_tail" : "fft_tail", a.L, K, a.nvec);
+    const size_t smem = tail_smem(K, a.vchunk);
+    switch (K) {
+#define LGK_CASE(k)                                                                                 \
+    case k:                                                                                         \
+        cudaFuncSetAttribute(k_fft_tail<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        LGK_LAUNCH(L, nmbuf, k_fft_tail<k, INV><<<blocks, 256, smem, L.stream>>>(a));               \
+        break;
+        LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
         default: return cudaErrorInvalidValue;
     }
@@ -199,6 +304,7 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
     for (uint32_t i = 0, d = 0; i < np; ++i) { d0s[i] = d; d += ks[i]; }
     uint32_t nvec_p2 = 1;
     while (nvec_p2 < nvec) nvec_p2 <<= 1;
+    const bool aligned = ((uintptr_t)data % 16 == 0) && (col_stride % 4 == 0) && (q_stride % 4 == 0);
     for (uint32_t pi = 0; pi < np; ++pi) {
         const uint32_t p = inverse ? np - 1 - pi : pi;
         const uint32_t K = ks[p], d0 = d0s[p];
@@ -206,7 +312,18 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
         a.data = data; a.tw = tw; a.col_stride = col_stride; a.q_stride = q_stride;
         a.L = log_len; a.d0 = d0; a.log_S = log_len - d0 - K;
         a.log_nvec_p2 = ilog2u(nvec_p2); a.nvec = nvec; a.root_base = root_base;
-        a.vec_ok = ((uintptr_t)data % 16 == 0) && (col_stride % 4 == 0) && (q_stride % 4 == 0);
+        a.vec_ok = aligned;
+        const bool tail = a.log_S == 0 && K >= 4 && aligned;
+        if (tail) {
+            a.vchunk = std::min<uint32_t>(nvec, 64);
+            a.nchunks = (nvec + a.vchunk - 1) / a.vchunk;
+            const uint64_t blocks = ((uint64_t)Q << d0) * a.nchunks;
+            if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+            cudaError_t e = inverse ? launch_tail<true>(L, (int)K, a, (unsigned)blocks)
+                                    : launch_tail<false>(L, (int)K, a, (unsigned)blocks);
+            if (e != cudaSuccess) return e;
+            continue;
+        }
         const uint64_t G = (uint64_t)nvec_p2 << a.log_S;  // threads per (q, P)
         const uint32_t B = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>(G, 256));
         a.log_B = ilog2u(B);
@@ -345,13 +462,14 @@ struct Coeffs64 { uint32_t v[64]; };
 // with gr the Lagrange (eq) basis of the k challenges; one table per gr[j].
 __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
                                                  uint64_t M, uint32_t nj, Coeffs64 gr) {
-    extern __shared__ uint32_t tabs[];
+    extern __shared__ __align__(128) uint8_t tabs8[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (uint32_t j = warp; j < nj; j += nw) tab_build_warp(tabs + j * kTabWords, gr.v[j], lane);
+    for (uint32_t j = warp; j < nj; j += nw)
+        tab_build_warp(reinterpret_cast<uint32_t *>(tabs8 + 512 * j), gr.v[j], lane);
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t acc = 0;
-        for (uint32_t j = 0; j < nj; ++j) acc ^= tab_mul(tabs + j * kTabWords, __ldg(in + j * M + i));
+        for (uint32_t j = 0; j < nj; ++j) acc ^= tab_mul_sa(tabs8, 512u * j, 0, __ldg(in + j * M + i));
         out[i] = acc;
     }
 }
@@ -413,15 +531,16 @@ cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t 
 __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__ f, const uint32_t *__restrict__ B,
                                                     uint64_t quarter, uint32_t r, uint32_t *__restrict__ fo,
                                                     uint32_t *__restrict__ Bo, uint32_t *acc3) {
-    __shared__ uint32_t T[kTabWords];
+    __shared__ __align__(128) uint32_t T[kTabWords];
     if (threadIdx.x < 32) tab_build_warp(T, r, threadIdx.x);
     __syncthreads();
+    const uint8_t *t8 = reinterpret_cast<const uint8_t *>(T);
     uint32_t s0 = 0, s1 = 0, s2 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < quarter; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t a0 = f[i], a1 = f[quarter + i], a2 = f[2 * quarter + i], a3 = f[3 * quarter + i];
         const uint32_t c0 = B[i], c1 = B[quarter + i], c2 = B[2 * quarter + i], c3 = B[3 * quarter + i];
-        const uint32_t flo = a0 ^ tab_mul(T, a0 ^ a2), fhi = a1 ^ tab_mul(T, a1 ^ a3);
-        const uint32_t blo = c0 ^ tab_mul(T, c0 ^ c2), bhi = c1 ^ tab_mul(T, c1 ^ c3);
+        const uint32_t flo = a0 ^ tab_mul_sa(t8, 0, 0, a0 ^ a2), fhi = a1 ^ tab_mul_sa(t8, 0, 0, a1 ^ a3);
+        const uint32_t blo = c0 ^ tab_mul_sa(t8, 0, 0, c0 ^ c2), bhi = c1 ^ tab_mul_sa(t8, 0, 0, c1 ^ c3);
         fo[i] = flo; fo[quarter + i] = fhi;
         Bo[i] = blo; Bo[quarter + i] = bhi;
         s0 ^= gf_mul(flo, blo);
@@ -441,11 +560,11 @@ cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32
 
 // glue (src/ligerito.rs:59-67) folded into the running basis sum
 __global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi, uint64_t n, uint32_t beta) {
-    __shared__ uint32_t T[kTabWords];
+    __shared__ __align__(128) uint32_t T[kTabWords];
     if (threadIdx.x < 32) tab_build_warp(T, beta, threadIdx.x);
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        B[i] ^= tab_mul(T, bi[i]);
+        B[i] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(T), 0, 0, bi[i]);
 }
 cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta) {
     const uint64_t n = 1ull << log_len;
@@ -473,6 +592,60 @@ InducePlan induce_plan(uint32_t n, uint32_t nq) {
     return p;
 }
 
+// Per-query setup of induce_sumcheck_poly_parallel, one block:
+//   dot_k = <row_k, gr> (rows gathered on the device), apow_k = alpha^k
+//   (precompute_alpha_powers, src/sumcheck_polys.rs:6-20),
+//   S_k[0] = q_k, S_k[i] = next_s(S_k[i-1], sks[i-1]) (sks_at_x,
+//   src/binary_fft.rs:289-292), and enforced_sum = sum_k apow_k * dot_k.
+struct InduceSetupArgs {
+    uint32_t gr[256];
+    uint32_t sks[32];
+};
+__global__ void k_induce_setup(const uint32_t *__restrict__ rows, uint32_t glen, const uint64_t *__restrict__ q,
+                               uint32_t nq, uint32_t alpha, uint32_t n, InduceSetupArgs args,
+                               uint32_t *__restrict__ S, uint32_t *__restrict__ apow, uint32_t *sum_out) {
+    uint32_t contrib = 0;
+    for (uint32_t k = threadIdx.x; k < nq; k += blockDim.x) {
+        uint32_t dot = 0;
+        for (uint32_t j = 0; j < glen; ++j) dot ^= gf_mul(rows[(uint64_t)k * glen + j], args.gr[j]);
+        uint32_t p = 1, base = alpha;
+        for (uint32_t e = k; e; e >>= 1) {
+            if (e & 1) p = gf_mul(p, base);
+            base = gf_mul(base, base);
+        }
+        apow[k] = p;
+        contrib ^= gf_mul(dot, p);
+        if (n) {
+            uint32_t sx = (uint32_t)q[k];
+            S[(uint64_t)k * n] = sx;
+            for (uint32_t i = 1; i < n; ++i) {
+                sx = gf_mul(sx, sx) ^ gf_mul(args.sks[i - 1], sx);
+                S[(uint64_t)k * n + i] = sx;
+            }
+        }
+    }
+    __shared__ uint32_t red;
+    if (threadIdx.x == 0) red = 0;
+    __syncthreads();
+    contrib = warp_xor(contrib);
+    if ((threadIdx.x & 31) == 0) atomicXor(&red, contrib);
+    __syncthreads();
+    if (threadIdx.x == 0) *sum_out = red;
+}
+
+cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
+                         const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
+                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum) {
+    if (glen > 256 || n > 32 || nq == 0) return cudaErrorInvalidValue;
+    InduceSetupArgs args{};
+    for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
+    for (uint32_t i = 0; i + 1 < n && i < 32; ++i) args.sks[i] = sks[i];
+    const unsigned threads = std::min<unsigned>(256, ((nq + 31) / 32) * 32);
+    LGK_LAUNCH(L, "induce_setup", k_induce_setup<<<1, threads, 0, L.stream>>>(d_rows, glen, d_q, nq, alpha, n, args,
+                                                                           d_S, d_apow, d_sum));
+    return cudaGetLastError();
+}
+
 __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__restrict__ apow, uint32_t n,
                               uint32_t b, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi) {
     const uint32_t k = blockIdx.x;
@@ -496,7 +669,7 @@ template <int ACC>  // ACC = max(1, 2^b / 32) words per lane
 __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
                                                      uint32_t n, uint32_t b, uint32_t nq, uint32_t qs,
                                                      uint32_t *__restrict__ out, int atomic_out) {
-    __shared__ uint32_t tabs[8][kTabWords];
+    __shared__ __align__(128) uint32_t tabs[8][kTabWords];
     __shared__ uint32_t red[32 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t tb = blockIdx.x, nlo = 1u << b, nhi = 1u << (n - b);
@@ -511,7 +684,7 @@ __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict_
 #pragma unroll
         for (int c = 0; c < ACC; ++c) {
             const uint32_t u = lane + 32 * c;
-            if (u < nlo) acc[c] ^= tab_mul(tabs[warp], __ldg(lk + u));
+            if (u < nlo) acc[c] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * warp, 0, __ldg(lk + u));
         }
         __syncwarp();
     }

@@ -80,6 +80,12 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
                          uint32_t n, uint32_t nq, uint32_t *d_scratch_lo, uint32_t *d_scratch_hi,
                          uint32_t *out);
 
+// Per-query inputs of induce_basis from device-resident opened rows
+// (nq x glen): S (nq x n), apow (nq) and the enforced sum (1 word).
+cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
+                         const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
+                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum);
+
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);
 
 }  // namespace lgk

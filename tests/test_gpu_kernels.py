@@ -14,7 +14,7 @@ def rand_u32(n):
 
 
 @pytest.mark.parametrize("log_n,batch", [(1, 3), (2, 5), (3, 1), (5, 7), (6, 3), (7, 2), (10, 4), (12, 3),
-                                         (13, 2), (16, 2)])
+                                         (13, 2), (16, 2), (8, 100), (10, 130), (4, 70)])
 def test_fft_ifft_match_oracle(lg, ref, ctx, log_n, batch):
     # fft / ifft, src/binary_fft.rs:4-28, every vector of a batch
     v = rand_u32(batch << log_n).reshape(batch, -1)
