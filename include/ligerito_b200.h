@@ -35,7 +35,8 @@ typedef enum lg_status {
     LG_ERR_VERIFY_PANIC = 5,     /* the reference verifier would have panicked */
     LG_ERR_PROVER_ASSERT = 6,    /* a prover-side assert of the reference failed */
     LG_ERR_NO_DEVICE = 7,        /* no CUDA device / library built without one */
-    LG_ERR_MALFORMED_PROOF = 8   /* proof bytes do not parse */
+    LG_ERR_MALFORMED_PROOF = 8,  /* proof bytes do not parse */
+    LG_ERR_EXCEEDS_STATIC_SCRATCH = 9 /* sizes beyond the fixed scratch of a *_noalloc call */
 } lg_status;
 
 /* Mirrors ProverConfig / VerifierConfig (src/data_structures.rs:9-30) without
@@ -175,6 +176,33 @@ lg_status lg_transcript_get_distinct_queries(lg_transcript *t, uint64_t n, uint6
 lg_status lg_merkle_verify(const uint8_t *root, const uint8_t *proof, uint64_t n_sib, uint64_t depth,
                            const uint8_t *leaves, const uint64_t *leaf_off, const uint64_t *queries,
                            uint64_t nq, int *ok);
+
+/* The same result as lg_induce_sumcheck_poly, for callers that cannot
+ * allocate device memory: their device memory is owned by another allocator
+ * that reserved it up front, or they run on a path that must not call
+ * cudaMalloc / cudaFree because those can synchronise the whole device.
+ * No counterpart in the reference (it is an allocation-free variant of the
+ * call above, not a reference interface).
+ *
+ * Inputs and outputs are the caller's device buffers: d_rows (nrows x
+ * 2^nch words, row-major), d_queries (nrows sorted row indices),
+ * d_basis_out (2^n words), d_enforced_sum (1 word); v_challenges stays on
+ * the host.  Work is queued on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream) and the call returns without waiting for it.
+ *
+ * Scratch comes from one fixed array of LG_NOALLOC_SCRATCH_BYTES in device
+ * memory, reserved when the library loads and held by every GPU that loads
+ * it until the process exits.  Limit: nrows <= 256 and n <= 20 (anything
+ * larger returns LG_ERR_EXCEEDS_STATIC_SCRATCH and queues no work).  The
+ * first call on a device looks up that device's copy of the array, so it
+ * should come before any stream capture.  All calls share the array: calls
+ * whose work overlaps on the GPU race on it, so order them on one stream or
+ * wait between them. */
+#define LG_NOALLOC_SCRATCH_BYTES (4u << 20)
+lg_status lg_induce_sumcheck_poly_noalloc(void *stream, uint32_t n, const uint32_t *d_rows, uint32_t nrows,
+                                          const uint32_t *v_challenges, uint32_t nch,
+                                          const uint64_t *d_queries, uint32_t alpha, uint32_t *d_basis_out,
+                                          uint32_t *d_enforced_sum);
 
 /* Seeded coefficient generator (SplitMix64; coefficient i = low 32 bits of
  * output i).  The reference draws unseeded rand::random (src/main.rs:25). */

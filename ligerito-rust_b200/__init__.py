@@ -46,6 +46,7 @@ STATUS = {
     6: "prover assertion failed",
     7: "no CUDA device",
     8: "malformed proof",
+    9: "sizes exceed the fixed scratch of an allocation-free call",
 }
 
 
@@ -122,6 +123,7 @@ def _load() -> ctypes.CDLL:
         "lg_transcript_get_distinct_queries": (i32, [P, u64, u64, P]),
         "lg_merkle_verify": (i32, [P, P, u64, u64, P, P, P, u64, P]),
         "lg_fill_splitmix_host": (None, [u64, P, u64]),
+        "lg_induce_sumcheck_poly_noalloc": (i32, [P, u32, P, u32, P, u32, P, u32, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

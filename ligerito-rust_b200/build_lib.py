@@ -15,7 +15,7 @@ import sys
 PKG = pathlib.Path(__file__).resolve().parent
 ROOT = PKG.parent
 OUT = PKG / "_build" / "liblgpu.so"
-SOURCES = [PKG / "csrc" / f for f in ("lg_api.cu", "lg_kernels.cu", "lg_host.cpp")]
+SOURCES = [PKG / "csrc" / f for f in ("lg_api.cu", "lg_kernels.cu", "lg_host.cpp", "lg_noalloc.cu")]
 DEPS = SOURCES + [PKG / "csrc" / f for f in ("lg_device.cuh", "lg_kernels.h", "lg_host.h")] + [
     ROOT / "include" / "ligerito_b200.h"
 ]

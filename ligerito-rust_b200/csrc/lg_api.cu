@@ -673,6 +673,7 @@ const char *lg_status_string(lg_status s) {
         case LG_ERR_PROVER_ASSERT: return "prover assertion failed";
         case LG_ERR_NO_DEVICE: return "no CUDA device";
         case LG_ERR_MALFORMED_PROOF: return "malformed proof";
+        case LG_ERR_EXCEEDS_STATIC_SCRATCH: return "sizes exceed the fixed scratch of an allocation-free call";
     }
     return "unknown status";
 }
