@@ -36,7 +36,8 @@ typedef enum lg_status {
     LG_ERR_PROVER_ASSERT = 6,    /* a prover-side assert of the reference failed */
     LG_ERR_NO_DEVICE = 7,        /* no CUDA device / library built without one */
     LG_ERR_MALFORMED_PROOF = 8,  /* proof bytes do not parse */
-    LG_ERR_EXCEEDS_STATIC_SCRATCH = 9 /* sizes beyond the fixed scratch of a *_noalloc call */
+    LG_ERR_EXCEEDS_STATIC_SCRATCH = 9, /* sizes beyond the fixed scratch of a *_noalloc call */
+    LG_ERR_TIMEOUT = 10                /* lg_server_wait: not finished within the timeout */
 } lg_status;
 
 /* Mirrors ProverConfig / VerifierConfig (src/data_structures.rs:9-30) without
@@ -110,6 +111,32 @@ lg_status lg_proof_deserialize(const uint8_t *buf, uint64_t len, lg_proof **out)
 void lg_proof_free(lg_proof *proof);
 /* ProofSize::proof_size, src/data_structures.rs:165-194 */
 lg_status lg_proof_size(const lg_proof *proof, uint64_t *bytes);
+
+/* ------------------------------------------------- batched / served proving
+ * Many proofs of uneven sizes on one GPU.  A server runs `workers`
+ * threads, each with its own context; requests are admitted FIFO when their
+ * device footprint fits hbm_budget_bytes (0 = no budget) next to the ones
+ * in flight, and each admitted request is proved by the next free worker,
+ * so proofs that arrive while others run start as soon as a worker and
+ * memory free up and their GPU work overlaps.  Every proof is the same
+ * bytes lg_prove gives alone.  (The reference proves one polynomial per
+ * call, src/prover.rs:15; these have no counterpart there.) */
+typedef struct lg_server lg_server;
+lg_status lg_server_create(int device, uint64_t hbm_budget_bytes, uint32_t workers, lg_server **out);
+/* copy_input = 1 copies a host polynomial so the caller may free it at
+ * once; otherwise (and always for device input) it must stay valid until
+ * lg_server_wait returns for this ticket. */
+lg_status lg_server_submit(lg_server *srv, const lg_config *cfg, const uint32_t *poly, uint64_t len,
+                           int poly_on_device, int copy_input, uint64_t *ticket);
+/* timeout_ms < 0 waits forever; LG_ERR_TIMEOUT leaves the ticket valid.
+ * latency_ms = submit -> done, queue_ms = submit -> start (may be NULL). */
+lg_status lg_server_wait(lg_server *srv, uint64_t ticket, int64_t timeout_ms, lg_proof **proof,
+                         double *latency_ms, double *queue_ms);
+lg_status lg_server_stats(lg_server *srv, uint64_t *completed, uint64_t *queued, uint64_t *in_flight_bytes);
+void lg_server_destroy(lg_server *srv); /* finishes queued work first */
+/* count proofs on `workers` concurrent contexts; out[i] as lg_prove */
+lg_status lg_prove_batch(int device, uint32_t workers, const lg_config *cfgs, const uint32_t *const *polys,
+                         const uint64_t *lens, int polys_on_device, uint32_t count, lg_proof **out);
 
 /* ----------------------------------------------------- kernel entry points
  * Device pointers belong to the context's device; work is issued on the

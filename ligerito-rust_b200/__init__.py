@@ -47,6 +47,7 @@ STATUS = {
     7: "no CUDA device",
     8: "malformed proof",
     9: "sizes exceed the fixed scratch of an allocation-free call",
+    10: "timed out",
 }
 
 
@@ -124,6 +125,12 @@ def _load() -> ctypes.CDLL:
         "lg_merkle_verify": (i32, [P, P, u64, u64, P, P, P, u64, P]),
         "lg_fill_splitmix_host": (None, [u64, P, u64]),
         "lg_induce_sumcheck_poly_noalloc": (i32, [P, u32, P, u32, P, u32, P, u32, P, P]),
+        "lg_server_create": (i32, [i32, u64, u32, P]),
+        "lg_server_submit": (i32, [P, P, P, u64, i32, i32, P]),
+        "lg_server_wait": (i32, [P, u64, ctypes.c_int64, P, P, P]),
+        "lg_server_stats": (i32, [P, P, P, P]),
+        "lg_server_destroy": (None, [P]),
+        "lg_prove_batch": (i32, [i32, u32, P, P, P, i32, u32, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -624,3 +631,78 @@ def splitmix_coeffs_device(seed: int, n: int, ctx: Optional[Context] = None):
     out = _empty_dev(n, ctx.device)
     _check(lib.lg_fill_splitmix(ctx.handle, seed, _dev_ptr(out), n), ctx)
     return out
+
+
+# ------------------------------------------------------- batched / serving
+class Server:
+    """Continuous-batching proof server (lg_server_*): `workers` concurrent
+    contexts on one GPU, FIFO admission under an HBM budget."""
+
+    def __init__(self, device: int = 0, workers: int = 4, hbm_budget_bytes: int = 0):
+        self.handle = ctypes.c_void_p()
+        _check(lib.lg_server_create(device, hbm_budget_bytes, workers, ctypes.byref(self.handle)))
+        self._keep = {}
+
+    def submit(self, config: ProverConfig, poly, copy_input: bool = False) -> int:
+        c = config.to_c()
+        t = ctypes.c_uint64()
+        if _is_torch(poly):
+            st = lib.lg_server_submit(self.handle, ctypes.byref(c), _dev_ptr(poly), poly.numel(), 1, 0, ctypes.byref(t))
+        else:
+            a = _u32(poly)
+            st = lib.lg_server_submit(self.handle, ctypes.byref(c), a.ctypes.data, a.size, 0, 1 if copy_input else 0,
+                                      ctypes.byref(t))
+            poly = a
+        _check(st)
+        if not copy_input or _is_torch(poly):
+            self._keep[t.value] = poly  # the server reads it until wait() returns
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """-> (FinalizedLigeritoProof, latency_ms, queue_ms)"""
+        h = ctypes.c_void_p()
+        lat, q = ctypes.c_double(), ctypes.c_double()
+        st = lib.lg_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(h), ctypes.byref(lat), ctypes.byref(q))
+        if st == 10:
+            return None
+        self._keep.pop(ticket, None)
+        _check(st)
+        return FinalizedLigeritoProof(h), float(lat.value), float(q.value)
+
+    def stats(self) -> dict:
+        c, q, b = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib.lg_server_stats(self.handle, ctypes.byref(c), ctypes.byref(q), ctypes.byref(b)))
+        return {"completed": c.value, "queued": q.value, "in_flight_bytes": b.value}
+
+    def close(self) -> None:
+        if self.handle:
+            lib.lg_server_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def prove_batch(configs: Sequence[ProverConfig], polys, workers: int = 4, device: int = 0) -> list:
+    """Prove many polynomials (uneven sizes) concurrently; same bytes as
+    `prover` on each alone."""
+    n = len(polys)
+    cfgs = (LgConfig * n)(*[c.to_c() for c in configs])
+    on_dev = 1 if n and _is_torch(polys[0]) else 0
+    keep = []
+    ptrs = (ctypes.c_void_p * n)()
+    lens = (ctypes.c_uint64 * n)()
+    for i, p in enumerate(polys):
+        if on_dev:
+            ptrs[i], lens[i] = _dev_ptr(p), p.numel()
+        else:
+            a = _u32(p)
+            keep.append(a)
+            ptrs[i], lens[i] = a.ctypes.data, a.size
+    out = (ctypes.c_void_p * n)()
+    _check(lib.lg_prove_batch(device, workers, cfgs, ptrs, lens, on_dev, n, out))
+    return [FinalizedLigeritoProof(ctypes.c_void_p(out[i])) for i in range(n)]

@@ -15,13 +15,13 @@ import sys
 PKG = pathlib.Path(__file__).resolve().parent
 ROOT = PKG.parent
 OUT = PKG / "_build" / "liblgpu.so"
-SOURCES = [PKG / "csrc" / f for f in ("lg_api.cu", "lg_kernels.cu", "lg_host.cpp", "lg_noalloc.cu")]
+SOURCES = [PKG / "csrc" / f for f in ("lg_api.cu", "lg_kernels.cu", "lg_host.cpp", "lg_noalloc.cu", "lg_serve.cpp")]
 DEPS = SOURCES + [PKG / "csrc" / f for f in ("lg_device.cuh", "lg_kernels.h", "lg_host.h")] + [
     ROOT / "include" / "ligerito_b200.h"
 ]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-shared", "-cudart", "static",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xcompiler", "-pthread", "-shared", "-cudart", "static",
 ]
 
 

@@ -674,6 +674,7 @@ const char *lg_status_string(lg_status s) {
         case LG_ERR_NO_DEVICE: return "no CUDA device";
         case LG_ERR_MALFORMED_PROOF: return "malformed proof";
         case LG_ERR_EXCEEDS_STATIC_SCRATCH: return "sizes exceed the fixed scratch of an allocation-free call";
+        case LG_ERR_TIMEOUT: return "timed out";
     }
     return "unknown status";
 }

@@ -1,0 +1,217 @@
+// Batched and served proving (lg_server_*, lg_prove_batch).
+//
+// A server owns `workers` threads, each with its own context (stream,
+// arenas, cached RS tables) on one device.  Requests queue FIFO and are
+// admitted when their device footprint fits the HBM budget next to the
+// requests already in flight; an admitted request is proved by the next
+// free worker, so requests that arrive while others run start as soon as a
+// worker and memory free up, and their kernels and host transcript work
+// overlap with the others'.  A server with one worker is the FIFO loop of
+// the plain prover.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ligerito_b200.h"
+#include "lg_host.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    lg_config cfg{};
+    const uint32_t *poly = nullptr;
+    uint64_t len = 0;
+    int on_device = 0;
+    std::vector<uint32_t> owned;  // copy of host input when asked for
+    uint64_t mem = 0;             // admission footprint
+    Clock::time_point t_submit, t_start, t_done;
+    bool done = false;
+    lg_status st = LG_OK;
+    lg_proof *proof = nullptr;
+};
+
+// Device bytes one proof holds at its peak: the input when it is on the
+// host, the first encoded matrix (16 bytes per coefficient) and its tree
+// (4 per coefficient), the folded vectors and the per-context arenas.
+uint64_t footprint(const lg_config &c, uint64_t len, int on_device) {
+    uint64_t b = 16 * len + 4 * len + (len >> c.initial_k) * 4 * 4 + (48ull << 20);
+    if (!on_device) b += 4 * len;
+    return b;
+}
+
+}  // namespace
+
+struct lg_server {
+    int device = 0;
+    uint64_t budget = 0, in_flight = 0;
+    std::vector<lg_ctx *> ctxs;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request *> pending;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
+    uint64_t next_id = 1, completed = 0;
+    bool stop = false;
+    Clock::time_point t0 = Clock::now();
+
+    void worker(lg_ctx *ctx) {
+        for (;;) {
+            Request *r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] {
+                    return stop || (!pending.empty() && (budget == 0 || pending.front()->mem + in_flight <= budget ||
+                                                         in_flight == 0));
+                });
+                if (stop && pending.empty()) return;
+                if (pending.empty()) continue;
+                r = pending.front();
+                pending.pop_front();
+                in_flight += r->mem;
+                r->t_start = Clock::now();
+            }
+            lg_proof *p = nullptr;
+            lg_status st = lg_prove(ctx, &r->cfg, r->poly, r->len, r->on_device, &p);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                in_flight -= r->mem;
+                r->st = st;
+                r->proof = p;
+                r->t_done = Clock::now();
+                r->done = true;
+                r->owned.clear();
+                r->owned.shrink_to_fit();
+                ++completed;
+            }
+            cv_done.notify_all();
+            cv_work.notify_all();
+        }
+    }
+};
+
+extern "C" {
+
+lg_status lg_server_create(int device, uint64_t hbm_budget_bytes, uint32_t workers, lg_server **out) {
+    if (!out || workers == 0 || workers > 256) return LG_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    auto *s = new (std::nothrow) lg_server;
+    if (!s) return LG_ERR_OUT_OF_MEMORY;
+    s->device = device;
+    s->budget = hbm_budget_bytes;
+    for (uint32_t i = 0; i < workers; ++i) {
+        lg_ctx *c = nullptr;
+        lg_status st = lg_ctx_create(device, 0, &c);
+        if (st != LG_OK) {
+            for (auto *x : s->ctxs) lg_ctx_destroy(x);
+            delete s;
+            return st;
+        }
+        s->ctxs.push_back(c);
+    }
+    for (auto *c : s->ctxs) s->threads.emplace_back([s, c] { s->worker(c); });
+    *out = s;
+    return LG_OK;
+}
+
+lg_status lg_server_submit(lg_server *s, const lg_config *cfg, const uint32_t *poly, uint64_t len,
+                           int poly_on_device, int copy_input, uint64_t *ticket) {
+    if (!s || !cfg || !poly || !ticket) return LG_ERR_INVALID_ARGUMENT;
+    lg_status st = lg::config_check(*cfg, len);
+    if (st != LG_OK) return st;
+    auto r = std::make_unique<Request>();
+    r->cfg = *cfg;
+    r->len = len;
+    r->on_device = poly_on_device;
+    if (copy_input && !poly_on_device) {
+        r->owned.assign(poly, poly + len);
+        r->poly = r->owned.data();
+    } else {
+        r->poly = poly;
+    }
+    r->mem = footprint(*cfg, len, poly_on_device);
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        *ticket = r->id;
+        s->pending.push_back(r.get());
+        s->reqs.emplace(r->id, std::move(r));
+    }
+    s->cv_work.notify_one();
+    return LG_OK;
+}
+
+lg_status lg_server_wait(lg_server *s, uint64_t ticket, int64_t timeout_ms, lg_proof **proof, double *latency_ms,
+                         double *queue_ms) {
+    if (!s || !proof) return LG_ERR_INVALID_ARGUMENT;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return LG_ERR_INVALID_ARGUMENT;
+    Request *r = it->second.get();
+    auto ready = [&] { return r->done; };
+    if (timeout_ms < 0) s->cv_done.wait(lk, ready);
+    else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return LG_ERR_TIMEOUT;
+    *proof = r->proof;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    if (queue_ms) *queue_ms = std::chrono::duration<double, std::milli>(r->t_start - r->t_submit).count();
+    lg_status st = r->st;
+    s->reqs.erase(it);
+    return st;
+}
+
+lg_status lg_server_stats(lg_server *s, uint64_t *completed, uint64_t *queued, uint64_t *in_flight_bytes) {
+    if (!s) return LG_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (completed) *completed = s->completed;
+    if (queued) *queued = s->pending.size();
+    if (in_flight_bytes) *in_flight_bytes = s->in_flight;
+    return LG_OK;
+}
+
+void lg_server_destroy(lg_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto &t : s->threads) t.join();
+    for (auto &kv : s->reqs)
+        if (kv.second->proof) lg_proof_free(kv.second->proof);
+    for (auto *c : s->ctxs) lg_ctx_destroy(c);
+    delete s;
+}
+
+lg_status lg_prove_batch(int device, uint32_t workers, const lg_config *cfgs, const uint32_t *const *polys,
+                         const uint64_t *lens, int polys_on_device, uint32_t count, lg_proof **out) {
+    if (!cfgs || !polys || !lens || !out) return LG_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i) out[i] = nullptr;
+    lg_server *s = nullptr;
+    lg_status st = lg_server_create(device, 0, std::max<uint32_t>(1, std::min(workers, count)), &s);
+    if (st != LG_OK) return st;
+    std::vector<uint64_t> tickets(count);
+    lg_status first = LG_OK;
+    for (uint32_t i = 0; i < count; ++i) {
+        st = lg_server_submit(s, &cfgs[i], polys[i], lens[i], polys_on_device, 0, &tickets[i]);
+        if (st != LG_OK) { first = st; tickets[i] = 0; }
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!tickets[i]) continue;
+        st = lg_server_wait(s, tickets[i], -1, &out[i], nullptr, nullptr);
+        if (st != LG_OK && first == LG_OK) first = st;
+    }
+    lg_server_destroy(s);
+    return first;
+}
+
+}  // extern "C"
