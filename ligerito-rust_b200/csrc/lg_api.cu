@@ -35,6 +35,8 @@ struct Code {  // ReedSolomonEncoding::new(m, 4m) tables, src/reed_solomon.rs:49
 struct lg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // host->device input copies overlapped with compute
+    cudaEvent_t copy_ev[8] = {};
     lgk::Launcher L;
     uint64_t budget = 0, in_use = 0;
     std::string err;
@@ -220,37 +222,6 @@ struct Scratch {
     }
 };
 
-// Host polynomial to the device: pinned memory is copied directly,
-// pageable memory in pipelined 4 MiB chunks through the pinned arena.
-void upload_poly(lg_ctx *c, Scratch &sc, uint32_t *d, const uint32_t *h, uint64_t len) {
-    const size_t bytes = len * 4;
-    cudaPointerAttributes attr{};
-    if (cudaPointerGetAttributes(&attr, h) == cudaSuccess && attr.type == cudaMemoryTypeHost) {
-        CK(c, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c->stream));
-        return;
-    }
-    cudaGetLastError();
-    constexpr size_t kChunk = 4u << 20;
-    uint8_t *slot[2] = {sc.pin(kChunk), sc.pin(kChunk)};
-    cudaEvent_t ev[2];
-    CK(c, cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-    CK(c, cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
-    bool used[2] = {false, false};
-    for (size_t off = 0, i = 0; off < bytes; off += kChunk, ++i) {
-        const size_t n = std::min(kChunk, bytes - off);
-        const int k = (int)(i & 1);
-        if (used[k]) CK(c, cudaEventSynchronize(ev[k]));
-        std::memcpy(slot[k], reinterpret_cast<const uint8_t *>(h) + off, n);
-        CK(c, cudaMemcpyAsync(reinterpret_cast<uint8_t *>(d) + off, slot[k], n, cudaMemcpyHostToDevice, c->stream));
-        CK(c, cudaEventRecord(ev[k], c->stream));
-        used[k] = true;
-    }
-    CK(c, cudaEventSynchronize(ev[0]));
-    CK(c, cudaEventSynchronize(ev[1]));
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
-}
-
 // ------------------------------------------------------------ commitment
 struct Witness {  // RecursiveLigeroWitness, src/data_structures.rs:32-40
     DBuf E;       // column-major encoded matrix, cols x rows
@@ -279,6 +250,66 @@ Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
     w.tree = DBuf(c, (2 * w.rows - 1) * 32);
     commit_into(c, d_poly, log_m, n, w.E.u32(), w.tree.u32());
     d2h(c, w.root, w.tree.u32() + 8 * (2 * w.rows - 2), 32);
+    return w;
+}
+
+// The first commitment of a proof whose polynomial is on the host: the
+// columns travel in groups of 16 on the copy stream; the compute stream
+// waits for each group and runs its scale-and-spread and the strided FFT
+// passes (which treat columns independently) while the next group is in
+// flight, then the last pass, the leaf hashes and the tree on all columns.
+Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_t *d_poly, uint32_t log_m,
+                         uint32_t n) {
+    const Code &code = get_code(c, log_m);
+    const uint64_t m = 1ull << log_m, rows = 4 * m;
+    Witness w;
+    w.rows = rows;
+    w.cols = n;
+    w.E = DBuf(c, rows * n * 4);
+    w.tree = DBuf(c, (2 * rows - 1) * 32);
+    cudaPointerAttributes attr{};
+    const bool pinned_src = cudaPointerGetAttributes(&attr, h_poly) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    const uint32_t group = n >= 32 ? 16 : n, ngroups = (n + group - 1) / group;
+    // staging for pageable input: two pinned chunks, reused after their copy
+    constexpr size_t kChunk = 4u << 20;
+    uint8_t *slot[2] = {nullptr, nullptr};
+    bool slot_busy[2] = {false, false};
+    int next_slot = 0;
+    if (!pinned_src) { slot[0] = sc.pin(kChunk); slot[1] = sc.pin(kChunk); }
+    // the copy stream must not start before work already queued on the
+    // compute stream that may still read d_poly's memory
+    CK(c, cudaEventRecord(c->copy_ev[7], c->stream));
+    CK(c, cudaStreamWaitEvent(c->copy_stream, c->copy_ev[7], 0));
+    for (uint32_t g = 0; g < ngroups; ++g) {
+        const uint32_t j0 = g * group, cols = std::min(group, n - j0);
+        const uint8_t *src = reinterpret_cast<const uint8_t *>(h_poly + (uint64_t)j0 * m);
+        uint8_t *dst = reinterpret_cast<uint8_t *>(d_poly + (uint64_t)j0 * m);
+        const size_t bytes = (size_t)cols * m * 4;
+        if (pinned_src) {
+            CK(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->copy_stream));
+        } else {
+            for (size_t off = 0; off < bytes; off += kChunk) {
+                const size_t nb = std::min(kChunk, bytes - off);
+                const int k = next_slot;
+                next_slot ^= 1;
+                if (slot_busy[k]) CK(c, cudaEventSynchronize(c->copy_ev[4 + k]));
+                std::memcpy(slot[k], src + off, nb);
+                CK(c, cudaMemcpyAsync(dst + off, slot[k], nb, cudaMemcpyHostToDevice, c->copy_stream));
+                CK(c, cudaEventRecord(c->copy_ev[4 + k], c->copy_stream));
+                slot_busy[k] = true;
+            }
+        }
+        CK(c, cudaEventRecord(c->copy_ev[g % 4], c->copy_stream));
+        CK(c, cudaStreamWaitEvent(c->stream, c->copy_ev[g % 4], 0));
+        uint32_t *Eg = w.E.u32() + (uint64_t)j0 * rows;
+        CK(c, lgk::rs_scale_spread(c->L, d_poly + (uint64_t)j0 * m, code.pis, Eg, log_m, cols));
+        CK(c, lgk::fft_vectors(c->L, Eg, code.tw, log_m, cols, rows, 4, m, 4, false, lgk::FFT_HEAD));
+    }
+    CK(c, lgk::fft_vectors(c->L, w.E.u32(), code.tw, log_m, n, rows, 4, m, 4, false, lgk::FFT_LAST));
+    CK(c, lgk::leaf_hashes(c->L, w.E.u32(), rows, n, w.tree.u32()));
+    CK(c, lgk::merkle_upper(c->L, w.tree.u32(), rows));
+    d2h(c, w.root, w.tree.u32() + 8 * (2 * rows - 2), 32);
     return w;
 }
 
@@ -375,12 +406,15 @@ void absorb3(lg::Transcript &fs, const std::array<uint32_t, 3> &s) { fs.absorb_u
 // each root, each round triple and yr, so those are the only device->host
 // reads inside the proof.  Openings are downloaded asynchronously and
 // materialised at the end.
-void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_poly, uint64_t len, lg::Proof &P) {
+void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_poly, uint64_t len, lg::Proof &P,
+                const uint32_t *h_poly = nullptr) {
     const size_t s = LG_NUM_QUERIES;
     lg::Transcript fs(LG_FS_SEED);
     uint32_t *acc = static_cast<uint32_t *>(sc.dev(16));  // s0, s1, s2, enforced sum
     uint32_t hacc[4];
-    Witness w0 = commit(c, d_poly, cfg.initial_log_m, 1u << cfg.initial_log_n);  // :32-37
+    Witness w0 = h_poly ? commit_from_host(c, sc, h_poly, const_cast<uint32_t *>(d_poly), cfg.initial_log_m,
+                                           1u << cfg.initial_log_n)
+                        : commit(c, d_poly, cfg.initial_log_m, 1u << cfg.initial_log_n);  // :32-37
     P.initial_root.assign(w0.root, w0.root + 32);
     fs.absorb(w0.root, 32);  // :48
 
@@ -742,6 +776,12 @@ lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
         delete c;
         return LG_ERR_CUDA;
     }
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return LG_ERR_CUDA;
+    }
+    for (auto &e : c->copy_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
         uint64_t thr = UINT64_MAX;
@@ -762,6 +802,8 @@ void lg_ctx_destroy(lg_ctx *c) {
     if (c->pin_arena) cudaFreeHost(c->pin_arena);
     if (c->dev_arena) cudaFree(c->dev_arena);
     c->L.release();
+    for (auto e : c->copy_ev) if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -813,8 +855,7 @@ lg_status lg_prove(lg_ctx *c, const lg_config *cfg, const uint32_t *poly, uint64
             prove_impl(c, sc, *cfg, poly, len, res->p);
         } else {
             DBuf d(c, len * 4);
-            upload_poly(c, sc, d.u32(), poly, len);
-            prove_impl(c, sc, *cfg, d.u32(), len, res->p);
+            prove_impl(c, sc, *cfg, d.u32(), len, res->p, poly);
         }
         sc.finish();
     });

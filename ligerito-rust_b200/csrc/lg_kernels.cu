@@ -294,7 +294,7 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
 
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse) {
+                        uint32_t root_base, bool inverse, FftPasses passes) {
     if (log_len == 0 || nvec == 0) return cudaSuccess;
     // split log_len stages into passes of <= 6, balanced
     const uint32_t np = (log_len + 5) / 6;
@@ -305,8 +305,10 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
     uint32_t nvec_p2 = 1;
     while (nvec_p2 < nvec) nvec_p2 <<= 1;
     const bool aligned = ((uintptr_t)data % 16 == 0) && (col_stride % 4 == 0) && (q_stride % 4 == 0);
+    if (inverse && passes != FFT_ALL) return cudaErrorInvalidValue;
     for (uint32_t pi = 0; pi < np; ++pi) {
         const uint32_t p = inverse ? np - 1 - pi : pi;
+        if ((passes == FFT_HEAD && p == np - 1) || (passes == FFT_LAST && p != np - 1)) continue;
         const uint32_t K = ks[p], d0 = d0s[p];
         PassArgs a;
         a.data = data; a.tw = tw; a.col_stride = col_stride; a.q_stride = q_stride;

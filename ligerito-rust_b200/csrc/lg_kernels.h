@@ -39,9 +39,13 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
 // vectors of 2^log_len: vector (j, q) starts at data + j*col_stride +
 // q*q_stride and uses the twiddle subtree under heap node root_base + q of
 // `tw` (heap order, tw[idx-1]).
+// passes: FFT_ALL, FFT_HEAD (every pass but the last), FFT_LAST (only the
+// last; forward only) -- the head passes treat vectors independently, so a
+// batch may run them in column groups and the last pass once for all.
+enum FftPasses { FFT_ALL = 0, FFT_HEAD = 1, FFT_LAST = 2 };
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse);
+                        uint32_t root_base, bool inverse, FftPasses passes = FFT_ALL);
 
 // --- Merkle (src/merkle_tree.rs:4-60, leaves src/ligero.rs:53-68) --------
 // Leaf hash of every row of a column-major matrix (rows x ncols u32).

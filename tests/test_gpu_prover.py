@@ -44,6 +44,20 @@ def test_config20_host_input_equals_device_input(lg, ctx, golden):
     assert lg.verifier(lg.hardcoded_config_20_verifier(), a, ctx)
 
 
+def test_pinned_and_pageable_host_inputs_give_the_same_proof(lg, ctx):
+    # the host paths overlap the input copy with the first commitment
+    import torch
+
+    cfg = lg.hardcoded_config_24()
+    poly = lg.splitmix_coeffs(1, 1 << 24)
+    pinned = torch.empty(1 << 24, dtype=torch.int32, pin_memory=True)
+    pinned.copy_(torch.from_numpy(poly.view(np.int32)))
+    a = lg.prover(cfg, pinned.numpy().view(np.uint32), ctx).to_bytes()
+    b = lg.prover(cfg, poly, ctx).to_bytes()
+    c = lg.prover(cfg, lg.to_device(poly), ctx).to_bytes()
+    assert a == b == c
+
+
 def test_config24_matches_oracle(lg, ref, ctx):
     # config 24 (src/config.rs:69-134), seed 1: byte-identical to the oracle
     import os
