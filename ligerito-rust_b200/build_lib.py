@@ -15,8 +15,9 @@ import sys
 PKG = pathlib.Path(__file__).resolve().parent
 ROOT = PKG.parent
 OUT = PKG / "_build" / "liblgpu.so"
-SOURCES = [PKG / "csrc" / f for f in ("lg_api.cu", "lg_kernels.cu", "lg_host.cpp", "lg_noalloc.cu", "lg_serve.cpp")]
-DEPS = SOURCES + [PKG / "csrc" / f for f in ("lg_device.cuh", "lg_kernels.h", "lg_host.h")] + [
+SOURCES = [PKG / "csrc" / f for f in ("lg_api.cu", "lg_kernels.cu", "lg_fs.cu", "lg_host.cpp", "lg_noalloc.cu",
+                                      "lg_serve.cpp")]
+DEPS = SOURCES + [PKG / "csrc" / f for f in ("lg_device.cuh", "lg_fs.cuh", "lg_kernels.h", "lg_host.h")] + [
     ROOT / "include" / "ligerito_b200.h"
 ]
 NVCC_FLAGS = [

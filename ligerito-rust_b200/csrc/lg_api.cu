@@ -228,7 +228,7 @@ struct Witness {  // RecursiveLigeroWitness, src/data_structures.rs:32-40
     DBuf tree;    // all layers, leaves first, 8 words per node
     uint64_t rows = 0;
     uint32_t cols = 0;
-    uint8_t root[32];
+    const uint32_t *root() const { return tree.u32() + 8 * (2 * rows - 2); }  // on the device
 };
 
 // ligero_commit (src/ligero.rs:70-95) into caller buffers
@@ -241,7 +241,6 @@ void commit_into(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, 
     CK(c, lgk::merkle_upper(c->L, tree, rows));
 }
 
-// commitment + its root on the host (the transcript needs it next)
 Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
     Witness w;
     w.rows = 4ull << log_m;
@@ -249,15 +248,17 @@ Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
     w.E = DBuf(c, w.rows * n * 4);
     w.tree = DBuf(c, (2 * w.rows - 1) * 32);
     commit_into(c, d_poly, log_m, n, w.E.u32(), w.tree.u32());
-    d2h(c, w.root, w.tree.u32() + 8 * (2 * w.rows - 2), 32);
     return w;
 }
 
 // The first commitment of a proof whose polynomial is on the host: the
 // columns travel in groups of 16 on the copy stream; the compute stream
-// waits for each group and runs its scale-and-spread and the strided FFT
-// passes (which treat columns independently) while the next group is in
-// flight, then the last pass, the leaf hashes and the tree on all columns.
+// waits for each group and, while the next group is in flight, encodes it
+// (scale-and-spread and FFT treat columns independently) and runs its
+// BLAKE3 block of every leaf: a leaf is the row's words in column order and
+// 16 words are one BLAKE3 block, so group g is block g of each leaf's
+// chunk, chained through the leaf slots of the tree.  After the last group
+// only the upper tree remains.
 Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_t *d_poly, uint32_t log_m,
                          uint32_t n) {
     const Code &code = get_code(c, log_m);
@@ -270,7 +271,7 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
     cudaPointerAttributes attr{};
     const bool pinned_src = cudaPointerGetAttributes(&attr, h_poly) == cudaSuccess && attr.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    const uint32_t group = n >= 32 ? 16 : n, ngroups = (n + group - 1) / group;
+    const uint32_t group = std::min<uint32_t>(n, 16), ngroups = (n + group - 1) / group;
     // staging for pageable input: two pinned chunks, reused after their copy
     constexpr size_t kChunk = 4u << 20;
     uint8_t *slot[2] = {nullptr, nullptr};
@@ -304,12 +305,10 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
         CK(c, cudaStreamWaitEvent(c->stream, c->copy_ev[g % 4], 0));
         uint32_t *Eg = w.E.u32() + (uint64_t)j0 * rows;
         CK(c, lgk::rs_scale_spread(c->L, d_poly + (uint64_t)j0 * m, code.pis, Eg, log_m, cols));
-        CK(c, lgk::fft_vectors(c->L, Eg, code.tw, log_m, cols, rows, 4, m, 4, false, lgk::FFT_HEAD));
+        CK(c, lgk::fft_vectors(c->L, Eg, code.tw, log_m, cols, rows, 4, m, 4, false));
+        CK(c, lgk::leaf_hash_block(c->L, w.E.u32(), rows, n, g, w.tree.u32()));
     }
-    CK(c, lgk::fft_vectors(c->L, w.E.u32(), code.tw, log_m, n, rows, 4, m, 4, false, lgk::FFT_LAST));
-    CK(c, lgk::leaf_hashes(c->L, w.E.u32(), rows, n, w.tree.u32()));
     CK(c, lgk::merkle_upper(c->L, w.tree.u32(), rows));
-    d2h(c, w.root, w.tree.u32() + 8 * (2 * rows - 2), 32);
     return w;
 }
 
@@ -345,19 +344,68 @@ std::pair<const uint32_t *, const uint64_t *> open_rows(lg_ctx *c, Scratch &sc, 
     return {d_out, d_idx};
 }
 
+// The same opening with the queries drawn by the device transcript:
+// fs_queries absorbs `absorb` (a root, 32 bytes), draws the distinct sorted
+// queries on w's rows and their multi-proof node list, then squeezes
+// `nsq` challenges into out.  Returns the device copy of the opened rows
+// and of the queries.
+std::pair<const uint32_t *, const uint64_t *> open_rows_dev(lg_ctx *c, Scratch &sc, const Witness &w,
+                                                            lgk::FsState *fs, const uint32_t *absorb, uint32_t nsq,
+                                                            uint32_t *out, lg::Opening *op) {
+    const uint32_t nq = LG_NUM_QUERIES;
+    uint32_t depth = 0;
+    while ((1ull << depth) < w.rows) ++depth;
+    const uint32_t cap = nq * std::max<uint32_t>(depth, 1);
+    uint64_t *d_q = static_cast<uint64_t *>(sc.dev(8ull * nq));
+    uint64_t *d_nodes = static_cast<uint64_t *>(sc.dev(8ull * cap));
+    uint32_t *d_out = static_cast<uint32_t *>(sc.dev((nq * w.cols + (size_t)cap * 8 + 1) * 4));
+    uint32_t *d_cnt = d_out + nq * w.cols + (size_t)cap * 8;
+    lgk::FsQueries a;
+    a.src = absorb;
+    a.nwords = 8;
+    a.n = w.rows;
+    a.s = nq;
+    a.q = d_q;
+    a.nodes = d_nodes;
+    a.nodes_cap = cap;
+    a.nnodes = d_cnt;
+    a.nsq = nsq;
+    a.out = out;
+    CK(c, lgk::fs_queries(c->L, fs, a));
+    CK(c, lgk::gather_rows(c->L, w.E.u32(), w.rows, w.cols, d_q, nq, d_out));
+    CK(c, lgk::gather_nodes(c->L, w.tree.u32(), d_nodes, cap, d_out + nq * w.cols, d_cnt));
+    const uint32_t *h = sc.download_later(d_out, nq * w.cols + (size_t)cap * 8 + 1);
+    const uint32_t cols = w.cols;
+    sc.finalizers.push_back([h, nq, cap, cols, op]() {
+        op->rows.resize(nq);
+        for (size_t k = 0; k < nq; ++k) op->rows[k].assign(h + k * cols, h + (k + 1) * cols);
+        const uint32_t nr = std::min(h[nq * cols + (size_t)cap * 8], cap);
+        op->merkle.resize(nr);
+        for (size_t i = 0; i < nr; ++i) {
+            const uint8_t *b = reinterpret_cast<const uint8_t *>(h + nq * cols + 8 * i);
+            op->merkle[i].assign(b, b + 32);
+        }
+    });
+    return {d_out, d_q};
+}
+
 // induce_sumcheck_poly_parallel (src/sumcheck_polys.rs:74-160) entirely on
 // the device from device-resident rows (nq x 2^nch) and queries; the
 // enforced sum lands in d_sum (1 word).
+// The challenges (vch, alpha) come from the host, or from the device as
+// d_vch / d_alpha.
 void induce_dev(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *d_rows, uint32_t nq, const uint32_t *vch,
-                uint32_t nch, const uint64_t *d_q, uint32_t alpha, uint32_t *d_out, uint32_t *d_sum) {
-    std::vector<uint32_t> gr = lg::lagrange_basis(vch, nch);
+                uint32_t nch, const uint64_t *d_q, uint32_t alpha, uint32_t *d_out, uint32_t *d_sum,
+                const uint32_t *d_vch = nullptr, const uint32_t *d_alpha = nullptr) {
+    std::vector<uint32_t> gr = d_vch ? std::vector<uint32_t>() : lg::lagrange_basis(vch, nch);
     std::vector<uint32_t> sks = lg::eval_sk_at_vks(1ull << n);
     lgk::InducePlan plan = lgk::induce_plan(n, nq);
     uint32_t *d_S = static_cast<uint32_t *>(sc.dev(4ull * nq * std::max<uint32_t>(n, 1)));
     uint32_t *d_apow = static_cast<uint32_t *>(sc.dev(4ull * nq));
     uint32_t *d_lo = static_cast<uint32_t *>(sc.dev(4ull * nq << plan.b));
     uint32_t *d_hi = static_cast<uint32_t *>(sc.dev(4ull * nq << (n - plan.b)));
-    CK(c, lgk::induce_setup(c->L, d_rows, 1u << nch, gr.data(), d_q, nq, alpha, n, sks.data(), d_S, d_apow, d_sum));
+    CK(c, lgk::induce_setup(c->L, d_rows, 1u << nch, d_vch ? nullptr : gr.data(), d_q, nq, alpha, n, sks.data(), d_S,
+                            d_apow, d_sum, d_vch, d_alpha));
     if (plan.needs_zero) CK(c, cudaMemsetAsync(d_out, 0, 4ull << n, c->stream));
     CK(c, lgk::induce_basis(c->L, plan, d_S, d_apow, n, nq, d_lo, d_hi, d_out));
 }
@@ -375,22 +423,23 @@ uint32_t induce_host_rows(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *ro
     return sum;
 }
 
-// partial_eval by any number of challenges, chunks of <= 6 per launch
+// partial_eval by any number of challenges (host rs, or device d_rs),
+// chunks of <= 6 per launch
 void partial_eval_dev(lg_ctx *c, const uint32_t *d_in, uint32_t log_len, const uint32_t *rs, uint32_t k,
-                      uint32_t *d_out) {
+                      uint32_t *d_out, const uint32_t *d_rs = nullptr) {
     DBuf tmp[2];
     const uint32_t *src = d_in;
     uint32_t cur = log_len, done = 0, which = 0;
     while (done < k) {
         const uint32_t kk = std::min<uint32_t>(6, k - done);
-        std::vector<uint32_t> gr = lg::lagrange_basis(rs + done, kk);
+        std::vector<uint32_t> gr = d_rs ? std::vector<uint32_t>() : lg::lagrange_basis(rs + done, kk);
         uint32_t *dst;
         if (done + kk == k) dst = d_out;
         else {
             tmp[which] = DBuf(c, 4ull << (cur - kk));
             dst = tmp[which].u32();
         }
-        CK(c, lgk::fold_eq(c->L, src, dst, cur, kk, gr.data()));
+        CK(c, lgk::fold_eq(c->L, src, dst, cur, kk, d_rs ? nullptr : gr.data(), d_rs ? d_rs + done : nullptr));
         src = dst;
         which ^= 1;
         cur -= kk;
@@ -398,93 +447,138 @@ void partial_eval_dev(lg_ctx *c, const uint32_t *d_in, uint32_t log_len, const u
     }
 }
 
-void absorb3(lg::Transcript &fs, const uint32_t *s) { fs.absorb_u32s(s, 3); }
 void absorb3(lg::Transcript &fs, const std::array<uint32_t, 3> &s) { fs.absorb_u32s(s.data(), 3); }
 
 // ------------------------------------------------------------------ prover
-// prover (src/prover.rs:15-199).  The transcript runs on the host; it needs
-// each root, each round triple and yr, so those are the only device->host
-// reads inside the proof.  Openings are downloaded asynchronously and
-// materialised at the end.
+// prover (src/prover.rs:15-199).  The transcript runs on the device
+// (lg_fs.cu) up to yr: each challenge is squeezed into device memory
+// right after what it depends on is absorbed, and the kernels read it from
+// there, so the whole proof is queued without a host round trip.  yr is
+// then downloaded with the transcript state and the host finishes the
+// transcript (absorbing yr is long serial hashing) and the last opening.
+// Roots, sumcheck triples and openings are downloaded asynchronously and
+// materialised at the end; a failed prover assertion flagged on the device
+// (src/ligerito.rs:35,52, get_distinct_queries) raises ProverAssert there.
 void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_poly, uint64_t len, lg::Proof &P,
                 const uint32_t *h_poly = nullptr) {
-    const size_t s = LG_NUM_QUERIES;
-    lg::Transcript fs(LG_FS_SEED);
-    uint32_t *acc = static_cast<uint32_t *>(sc.dev(16));  // s0, s1, s2, enforced sum
-    uint32_t hacc[4];
+    const uint32_t steps = cfg.recursive_steps;
+    uint32_t nrounds = 0;
+    for (uint32_t i = 0; i < steps; ++i) nrounds += cfg.ks[i];
+    const uint32_t ntri = 1 + nrounds + (steps - 1);  // sumcheck triples, in transcript order
+    auto *fs = static_cast<lgk::FsState *>(sc.dev(sizeof(lgk::FsState)));
+    uint32_t *chal = static_cast<uint32_t *>(sc.dev(4ull * (cfg.initial_k + nrounds + 3 * steps + 4)));
+    // s0, s1, s2, enforced sum per triple, then the fused steps' block ticket
+    uint32_t *tri = static_cast<uint32_t *>(sc.dev(16ull * ntri + 16));
+    uint32_t *ticket = tri + 4 * ntri;
+    uint32_t nchal = 0, ntri_used = 0;
+    auto next_chal = [&](uint32_t n) { uint32_t *p = chal + nchal; nchal += n; return p; };
+    auto next_tri = [&]() { return tri + 4 * ntri_used++; };
+    CK(c, cudaMemsetAsync(tri, 0, 16ull * ntri + 16, c->stream));
+    CK(c, lgk::fs_init(c->L, fs, LG_FS_SEED));
+    auto root_later = [&](const Witness &w, std::vector<uint8_t> *dst) {
+        const uint32_t *h = sc.download_later(w.root(), 8);
+        sc.finalizers.push_back([h, dst]() {
+            const uint8_t *b = reinterpret_cast<const uint8_t *>(h);
+            dst->assign(b, b + 32);
+        });
+    };
+    auto tail = [&](bool check, uint32_t nsq, uint32_t *out) {
+        lgk::FsTail a;
+        a.fs = fs;
+        a.ticket = ticket;
+        a.check = check;
+        a.nsq = nsq;
+        a.out = out;
+        return a;
+    };
+    auto step = [&](const uint32_t *src, uint32_t nwords, bool check, uint32_t nsq, uint32_t *out) {
+        lgk::FsStep a;
+        a.src = src;
+        a.nwords = nwords;
+        a.check = check;
+        a.nsq = nsq;
+        a.out = out;
+        CK(c, lgk::fs_step(c->L, fs, a));
+    };
+
     Witness w0 = h_poly ? commit_from_host(c, sc, h_poly, const_cast<uint32_t *>(d_poly), cfg.initial_log_m,
                                            1u << cfg.initial_log_n)
                         : commit(c, d_poly, cfg.initial_log_m, 1u << cfg.initial_log_n);  // :32-37
-    P.initial_root.assign(w0.root, w0.root + 32);
-    fs.absorb(w0.root, 32);  // :48
-
-    P.recursive.reserve(cfg.recursive_steps);  // openings are filled in by pointer later
-    std::vector<uint32_t> pe0(cfg.initial_k);
-    for (auto &r : pe0) r = fs.get_field();  // :50
-    uint32_t fv = cfg.initial_log_m;         // log2 |f|
+    root_later(w0, &P.initial_root);
+    P.recursive_roots.resize(steps);
+    P.recursive.resize(steps - 1);  // openings are filled in by pointer later
+    const uint32_t *pe0 = next_chal(cfg.initial_k);
+    step(w0.root(), 8, false, cfg.initial_k, const_cast<uint32_t *>(pe0));  // :48-50
+    uint32_t fv = cfg.initial_log_m;  // log2 |f|
     DBuf f(c, 4ull << fv);
-    partial_eval_dev(c, d_poly, cfg.initial_log_m + cfg.initial_log_n, pe0.data(), cfg.initial_k, f.u32());  // :52-53
+    partial_eval_dev(c, d_poly, cfg.initial_log_m + cfg.initial_log_n, nullptr, cfg.initial_k, f.u32(), pe0);  // :52-53
 
     Witness wprev = commit(c, f.u32(), cfg.log_m[0], 1u << cfg.log_n[0]);  // :55-60
-    fs.absorb(wprev.root, 32);                                             // :64
-    P.recursive_roots.push_back(std::vector<uint8_t>(wprev.root, wprev.root + 32));
-
-    std::vector<uint64_t> q;
-    if (!fs.get_distinct_queries(w0.rows, s, q)) throw ProverAssert{};  // :67
-    const uint32_t alpha = fs.get_field();                             // :68
-    auto opened = open_rows(c, sc, w0, q, &P.initial);                 // :72-76
+    root_later(wprev, &P.recursive_roots[0]);
+    uint32_t *alpha = next_chal(1);
+    auto opened = open_rows_dev(c, sc, w0, fs, wprev.root(), 1, alpha, &P.initial);  // :64-76
     DBuf B(c, 4ull << fv);
-    CK(c, cudaMemsetAsync(acc, 0, 16, c->stream));
-    induce_dev(c, sc, fv, opened.first, (uint32_t)s, pe0.data(), cfg.initial_k, opened.second, alpha, B.u32(),
-               acc + 3);  // :78-85
+    uint32_t *t = next_tri();
+    induce_dev(c, sc, fv, opened.first, LG_NUM_QUERIES, nullptr, cfg.initial_k, opened.second, 0, B.u32(), t + 3, pe0,
+               alpha);  // :78-85
     w0.E.reset();
     w0.tree.reset();
-    CK(c, lgk::eval013(c->L, f.u32(), B.u32(), fv, acc));  // SumcheckProverInstance::new
-    d2h(c, hacc, acc, 16);
-    if ((hacc[0] ^ hacc[1]) != hacc[3]) throw ProverAssert{};  // src/ligerito.rs:35
-    P.transcript.push_back({hacc[0], hacc[1], hacc[2]});
-    absorb3(fs, hacc);  // :93
+    uint32_t *r = next_chal(1);
+    // SumcheckProverInstance::new, then :93 (src/ligerito.rs:35) and the
+    // first challenge of :97
+    const lgk::FsTail t0 = tail(true, 1, r);
+    CK(c, lgk::eval013(c->L, f.u32(), B.u32(), fv, t, &t0));
 
     DBuf f2(c, 4ull << (fv - 1)), B2(c, 4ull << (fv - 1));
-    for (uint32_t i = 0; i < cfg.recursive_steps; ++i) {
-        std::vector<uint32_t> rs;
-        for (uint32_t t = 0; t < cfg.ks[i]; ++t) {  // :97-102
-            const uint32_t r = fs.get_field();
-            CK(c, cudaMemsetAsync(acc, 0, 12, c->stream));
-            CK(c, lgk::fold_round(c->L, f.u32(), B.u32(), fv, r, f2.u32(), B2.u32(), acc));
+    for (uint32_t i = 0; i < steps; ++i) {
+        const uint32_t *rs = r;  // this step's ks[i] round challenges are consecutive
+        for (uint32_t k = 0; k < cfg.ks[i]; ++k) {  // :97-102
+            t = next_tri();
+            const bool more = k + 1 < cfg.ks[i];
+            uint32_t *rn = more ? next_chal(1) : nullptr;
+            const lgk::FsTail tk = tail(false, more ? 1 : 0, rn);
+            CK(c, lgk::fold_round(c->L, f.u32(), B.u32(), fv, 0, f2.u32(), B2.u32(), t, r, &tk));
             std::swap(f, f2);
             std::swap(B, B2);
             fv -= 1;
-            d2h(c, hacc, acc, 12);
-            P.transcript.push_back({hacc[0], hacc[1], hacc[2]});
-            absorb3(fs, hacc);
-            rs.push_back(r);
+            r = rn;
         }
-        if (i == cfg.recursive_steps - 1) {  // :104-143
+        if (i == steps - 1) {  // :104-143
             P.yr.resize(1ull << fv);
-            d2h(c, P.yr.data(), f.p, 4ull << fv);
-            fs.absorb_u32s(P.yr.data(), P.yr.size());
-            if (!fs.get_distinct_queries(wprev.rows, s, q)) throw ProverAssert{};
+            const uint32_t *hy = sc.download_later(f.u32(), 1ull << fv);
+            const lgk::FsState *hs = sc.download_later(fs, 1);
+            const uint32_t *ht = sc.download_later(tri, 4ull * ntri);
+            sc.finish();
+            std::memcpy(P.yr.data(), hy, 4ull << fv);
+            for (uint32_t j = 0; j < ntri; ++j) P.transcript.push_back({ht[4 * j], ht[4 * j + 1], ht[4 * j + 2]});
+            if (hs->err) throw ProverAssert{};
+            lg::Transcript fsh(LG_FS_SEED);
+            std::memcpy(fsh.h.h, hs->h, sizeof hs->h);
+            for (uint32_t k = 0; k < hs->nw && k < 16; ++k)
+                for (int b = 0; b < 4; ++b) fsh.h.buf[4 * k + b] = (uint8_t)(hs->w[k] >> (24 - 8 * b));
+            fsh.h.total = hs->total;
+            fsh.h.n = 4 * hs->nw;
+            fsh.counter = hs->counter;
+            fsh.absorb_u32s(P.yr.data(), P.yr.size());
+            std::vector<uint64_t> q;
+            if (!fsh.get_distinct_queries(wprev.rows, LG_NUM_QUERIES, q)) throw ProverAssert{};
             open_rows(c, sc, wprev, q, &P.final_);
             return;
         }
         Witness wn = commit(c, f.u32(), cfg.log_m[i + 1], 1u << cfg.log_n[i + 1]);  // :145-155
-        fs.absorb(wn.root, 32);
-        P.recursive_roots.push_back(std::vector<uint8_t>(wn.root, wn.root + 32));
-        if (!fs.get_distinct_queries(wprev.rows, s, q)) throw ProverAssert{};  // :157
-        const uint32_t al = fs.get_field();                                  // :158
-        P.recursive.emplace_back();
-        auto op = open_rows(c, sc, wprev, q, &P.recursive.back());  // :161-172
+        root_later(wn, &P.recursive_roots[i + 1]);
+        uint32_t *al = next_chal(1);
+        auto op = open_rows_dev(c, sc, wprev, fs, wn.root(), 1, al, &P.recursive[i]);  // :156-172
         DBuf bi(c, 4ull << fv);
-        CK(c, cudaMemsetAsync(acc, 0, 16, c->stream));
-        induce_dev(c, sc, fv, op.first, (uint32_t)s, rs.data(), cfg.ks[i], op.second, al, bi.u32(), acc + 3);
-        CK(c, lgk::eval013(c->L, f.u32(), bi.u32(), fv, acc));  // introduce_new
-        d2h(c, hacc, acc, 16);
-        if ((hacc[0] ^ hacc[1]) != hacc[3]) throw ProverAssert{};  // src/ligerito.rs:52
-        P.transcript.push_back({hacc[0], hacc[1], hacc[2]});
-        absorb3(fs, hacc);  // :187-191
-        const uint32_t beta = fs.get_field();  // :193
-        CK(c, lgk::axpy(c->L, B.u32(), bi.u32(), fv, beta));  // glue
+        t = next_tri();
+        induce_dev(c, sc, fv, op.first, LG_NUM_QUERIES, nullptr, cfg.ks[i], op.second, 0, bi.u32(), t + 3, rs, al);
+        // introduce_new, :187-193 (src/ligerito.rs:52): the glue challenge,
+        // then the next step's first round challenge
+        uint32_t *beta = next_chal(2);
+        const lgk::FsTail ti = tail(true, 2, beta);
+        CK(c, lgk::eval013(c->L, f.u32(), bi.u32(), fv, t, &ti));
+        r = beta + 1;
+        CK(c, lgk::axpy(c->L, B.u32(), bi.u32(), fv, 0, beta));  // glue
         wprev = std::move(wn);
     }
     throw ProverAssert{};  // :198
@@ -781,6 +875,13 @@ lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
         delete c;
         return LG_ERR_CUDA;
     }
+    if (cudaMalloc((void **)&c->L.dtab, lgk::kDtabWords * 4) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(c->copy_stream);
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return LG_ERR_OUT_OF_MEMORY;
+    }
     for (auto &e : c->copy_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -801,6 +902,7 @@ void lg_ctx_destroy(lg_ctx *c) {
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->pin_arena) cudaFreeHost(c->pin_arena);
     if (c->dev_arena) cudaFree(c->dev_arena);
+    if (c->L.dtab) cudaFree(c->L.dtab);
     c->L.release();
     for (auto e : c->copy_ev) if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);

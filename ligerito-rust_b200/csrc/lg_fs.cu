@@ -1,0 +1,212 @@
+// Fiat-Shamir transcript on the device: the prover's challenges, queries
+// and Merkle opening lists come from here, so a proof runs as one stream
+// of kernels without host round trips.
+//
+// The transcript (src/emulated_fs.rs:6-76) is a running SHA-256 (sha2
+// 0.10.9, FIPS 180-4): absorb appends bytes; squeeze appends the LE u32
+// counter, increments it and finalises a clone of the state; a field
+// element is the low 32 bits of the digest's first 16 bytes read as a LE
+// u128, a query the low 64 bits mod n.  get_distinct_queries rejects
+// repeats and sorts.  Everything absorbed is whole u32s, so the pending
+// message is kept as big-endian words.
+//
+// Absorbing is serial (one thread).  Squeezes are batched: squeeze i of a
+// batch finalises the state after i+1 more counters, so one thread
+// compresses the full blocks those counters complete (the only serial
+// part), then every thread finalises its own clone in parallel.
+#include <cstdint>
+
+#include "lg_fs.cuh"
+
+namespace lgk {
+
+namespace {
+
+using namespace fsd;
+
+__global__ void k_fs_init(FsState *g, uint32_t seed) {
+    __shared__ FsState S;
+    if (threadIdx.x == 0) {
+        const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                                0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+        for (int k = 0; k < 8; ++k) S.h[k] = iv[k];
+        S.nw = 0;
+        S.total = 0;
+        S.counter = 0;
+        S.err = 0;
+        S.pad = 0;
+        fs_absorb(S, &seed, 1);  // FS::new(seed): the seed's LE bytes
+    }
+    store_state(S, g);
+}
+
+__global__ void k_fs_step(FsState *g, FsStep a) {
+    __shared__ FsState S;
+    __shared__ Batch B;
+    load_state(S, g);
+    if (threadIdx.x == 0) {
+        if (a.check && (a.src[0] ^ a.src[1]) != a.src[3]) S.err |= FS_ERR_SUMCHECK;
+        fs_absorb(S, a.src, a.nwords);
+    }
+    __syncthreads();
+    fs_fields(S, B, a.nsq, a.out);
+    store_state(S, g);
+}
+
+// Exclusive prefix count of `flag` over the block (kQBlock threads) and
+// the total; `scratch` holds kQBlock / 32 words.
+__device__ uint32_t block_rank(bool flag, uint32_t *scratch, uint32_t *total) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t m = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) scratch[warp] = __popc(m);
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+    for (uint32_t w = 0; w < kQBlock / 32; ++w) {
+        const uint32_t c = scratch[w];
+        before += w < warp ? c : 0;
+        all += c;
+    }
+    __syncthreads();
+    *total = all;
+    return before + __popc(m & ((1u << lane) - 1));
+}
+
+__global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a) {
+    __shared__ FsState S;
+    __shared__ Batch B;
+    __shared__ uint64_t acc[kQBlock], cand[kQBlock];
+    __shared__ uint32_t lo32[kQBlock];
+    __shared__ uint32_t scratch[kQBlock / 32];
+    __shared__ uint32_t take_sh, batch_sh;
+    const uint32_t tid = threadIdx.x;
+    load_state(S, g);
+    if (tid == 0) fs_absorb(S, a.src, a.nwords);
+    __syncthreads();
+    const bool ok = a.n >= a.s && a.s >= 1 && a.s <= kQBlock;
+    const uint64_t mask = a.n - 1;  // n is a power of two: % n is a mask
+    uint32_t count = 0, batch = 0, take = 0;
+    // get_distinct_queries in batches of squeezes; the round bound only
+    // guards a state that cannot progress (n >= s always can)
+    for (uint32_t round = 0; ok && count < a.s && round < 1024; ++round) {
+        // a few more squeezes than queries still needed plus the challenges
+        // squeezed after them: the chain of full blocks a batch completes
+        // is its serial part
+        const uint32_t need = a.s - count;
+        batch = min(kQBlock, need + need / 16 + 8 + a.nsq);
+        if (tid == 0) fs_chain(S, B, batch);
+        __syncthreads();
+        uint64_t qv = 0;
+        if (tid < batch) {
+            const uint64_t lo = fs_squeeze_at(S, B, tid);
+            lo32[tid] = (uint32_t)lo;
+            qv = lo & mask;
+        }
+        cand[tid] = qv;
+        __syncthreads();
+        bool dup = tid >= batch;
+        for (uint32_t k = 0; k < count; ++k) dup |= acc[k] == qv;
+        for (uint32_t j = 0; j < tid; ++j) dup |= cand[j] == qv;
+        uint32_t fresh;
+        const uint32_t rank = block_rank(!dup, scratch, &fresh);
+        if (!dup && rank < need) acc[count + rank] = qv;
+        // squeezes consumed: the whole batch, or up to the one that
+        // completes the set
+        if (tid == 0) take_sh = batch;
+        __syncthreads();
+        if (fresh >= need && !dup && rank == need - 1) take_sh = tid + 1;
+        __syncthreads();
+        take = take_sh;
+        count += min(fresh, need);
+        // the challenges after the last query are the next squeezes of this
+        // batch when it has them; commit past those too
+        const uint32_t extra = count == a.s && take + a.nsq <= batch ? a.nsq : 0;
+        if (tid < extra) a.out[tid] = lo32[take + tid];
+        if (tid == 0) {
+            fs_commit(S, B, take + extra);
+            batch_sh = extra;
+        }
+        __syncthreads();
+    }
+    const uint32_t done_extra = ok && count == a.s ? batch_sh : 0;
+    if (!ok || count < a.s) {
+        if (tid == 0) {
+            S.err |= FS_ERR_QUERIES;
+            *a.nnodes = 0;
+        }
+        for (uint32_t i = tid; i < a.s && i < kQBlock; i += blockDim.x) a.q[i] = 0;
+    } else {
+        if (tid >= count) acc[tid] = ~0ull;
+        __syncthreads();
+        // bitonic sort of the kQBlock keys, one pair per thread per step
+        for (uint32_t size = 2; size <= kQBlock; size <<= 1)
+            for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+                const uint32_t i = tid, j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const uint64_t x = acc[i], y = acc[j];
+                    if ((x > y) == up) { acc[i] = y; acc[j] = x; }
+                }
+                __syncthreads();
+            }
+        if (tid < count) a.q[tid] = acc[tid];
+        // Multi-proof siblings (merkle_tree::prove, src/merkle_tree.rs:62-111):
+        // at layer d the present nodes are x = q >> d; the sibling x ^ 1 is
+        // emitted, in order of x, unless it is present too.  Queries are
+        // sorted, so the nodes equal to x form a run and x's sibling can only
+        // be the run's neighbour: an odd x is settled at its run's first
+        // query by the previous query, an even x at its run's last query by
+        // the next one.  Thread i owns query i across all layers.
+        const bool have = tid < count;
+        const uint64_t qi = have ? acc[tid] : 0;
+        const uint64_t qp = have && tid > 0 ? acc[tid - 1] : ~0ull;
+        const uint64_t qn = have && tid + 1 < count ? acc[tid + 1] : ~0ull;
+        uint32_t nout = 0;
+        uint64_t layer_off = 0, width = a.n;
+        for (uint32_t d = 0; (1ull << d) < a.n; ++d) {
+            bool emit = false;
+            uint64_t x = 0;
+            if (have) {
+                x = qi >> d;
+                const bool has_p = qp != ~0ull, has_n = qn != ~0ull;
+                const uint64_t xp = qp >> d, xn = qn >> d;
+                if (x & 1) emit = (!has_p || xp != x) && !(has_p && xp == (x ^ 1));
+                else emit = (!has_n || xn != x) && !(has_n && xn == (x ^ 1));
+            }
+            uint32_t tot;
+            const uint32_t pos = nout + block_rank(emit, scratch, &tot);
+            if (emit && pos < a.nodes_cap) a.nodes[pos] = layer_off + (x ^ 1);
+            nout += tot;
+            layer_off += width;
+            width >>= 1;
+        }
+        if (tid == 0) {
+            *a.nnodes = nout;
+            if (nout > a.nodes_cap) S.err |= FS_ERR_QUERIES;
+        }
+    }
+    __syncthreads();
+    if (done_extra < a.nsq) fs_fields(S, B, a.nsq - done_extra, a.out + done_extra);
+    store_state(S, g);
+}
+
+}  // namespace
+
+cudaError_t fs_init(Launcher &L, FsState *d, uint32_t seed) {
+    LGK_LAUNCH(L, "fs_init", k_fs_init<<<1, 32, 0, L.stream>>>(d, seed));
+    return cudaGetLastError();
+}
+
+cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a) {
+    if (a.nwords > 1024 || a.nsq > 256 || (a.check && (!a.src || a.nwords < 3))) return cudaErrorInvalidValue;
+    LGK_LAUNCH(L, "fs_step", k_fs_step<<<1, 32, 0, L.stream>>>(d, a));
+    return cudaGetLastError();
+}
+
+cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a) {
+    if (a.s == 0 || a.s > kQBlock || a.n == 0 || (a.n & (a.n - 1)) || a.nwords > 1024 || a.nsq > kQBlock)
+        return cudaErrorInvalidValue;
+    LGK_LAUNCH(L, "fs_queries", k_fs_queries<<<1, kQBlock, 0, L.stream>>>(d, a));
+    return cudaGetLastError();
+}
+
+}  // namespace lgk

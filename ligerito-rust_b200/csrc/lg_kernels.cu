@@ -1,6 +1,7 @@
 // CUDA kernels of liblgpu (sm_100a).  All arithmetic is exact GF(2^32) /
 // BLAKE3 integer work; there is no floating point and no tensor-core shape.
 #include "lg_device.cuh"
+#include "lg_fs.cuh"
 #include "lg_kernels.h"
 
 #include <algorithm>
@@ -53,13 +54,6 @@ void Launcher::release() {
     free_events.clear();
 }
 
-#define LGK_LAUNCH(L, name, ...)                  \
-    do {                                          \
-        cudaEvent_t _ev = nullptr;                \
-        (L).begin(name, &_ev);                    \
-        __VA_ARGS__;                              \
-        (L).end(name, _ev);                       \
-    } while (0)
 
 static inline unsigned ilog2u(uint64_t x) { unsigned r = 0; while (x > 1) { x >>= 1; ++r; } return r; }
 
@@ -95,26 +89,58 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
 struct PassArgs {
     uint32_t *data;
     const uint32_t *tw;
+    const uint4 *dtab;  // this pass's D tables (see build_pass_tables)
     uint64_t col_stride, q_stride;
     uint32_t L, d0, log_S, log_nvec_p2, nvec, log_bpg, log_B, root_base;
-    uint32_t vec_ok;            // 16-byte loads/stores allowed when a pencil is contiguous
-    uint32_t vchunk, nchunks;   // tail kernel: vectors per block, blocks per (q, P)
+    uint32_t vchunk, nchunks;  // last pass: vectors per block; both: blocks per (q, P)
 };
 
-// Builds the 2^K - 1 node tables of one (q, P) in 512-byte slots at the
-// start of `sm` (tab_mul_sa needs table offsets that are multiples of 256
-// relative to the array); returns the offset of slot 0.
+// The 2^K - 1 node tables of one (q, P), in 512-byte slots at the start of
+// `sm` (slot 2^s - 1 + t for node t of in-pass stage s).
+//
+// A heap layer of twiddles is GF(2)-linear in the node's offset within
+// the layer (compute_twiddles fills each layer by XOR from its basis,
+// src/binary_fft.rs:30-58).  The node offsets of the group's stage-s nodes
+// are (group offset << s) | t, so node t has twiddle C_s ^ D_{s,t}: C_s =
+// the twiddle of the group's first node at that stage, D_{s,t} = the
+// layer's value at offset t, the same for every group of the launch.  A
+// multiplication table is linear in its constant too: the block builds the
+// K tables of C_s (slot 2^s - 1, where t = 0 and D = 0) and XORs each other
+// slot from D's table (k_fft_dtab, once per launch), 4 words per access.
+// Ends with the block synchronised.
 template <int K>
-__device__ __forceinline__ uint32_t build_pass_tables(uint8_t *sm, const PassArgs &a, unsigned q, unsigned P) {
-    const uint32_t toff = 0;
+__device__ __forceinline__ void build_pass_tables(uint8_t *sm, const PassArgs &a, unsigned q, unsigned P) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint64_t hbase = ((uint64_t)(a.root_base + q) << a.d0) + P;
-    for (int slot = warp; slot < (1 << K) - 1; slot += nw) {
-        const int s = 31 - __clz(slot + 1);
-        const uint64_t heap = (hbase << s) + (uint64_t)(slot + 1 - (1 << s));
-        tab_build_warp(reinterpret_cast<uint32_t *>(sm + toff + slot * 512), __ldg(a.tw + heap - 1), lane);
+    for (int s = warp; s < K; s += nw)
+        tab_build_warp(reinterpret_cast<uint32_t *>(sm + ((1 << s) - 1) * 512), __ldg(a.tw + (hbase << s) - 1), lane);
+    __syncthreads();
+    uint4 *T = reinterpret_cast<uint4 *>(sm);
+    for (int i = threadIdx.x; i < ((1 << K) - 1) * 32; i += blockDim.x) {
+        const int slot = i >> 5, s = 31 - __clz(slot + 1), first = (1 << s) - 1;
+        if (slot == first) continue;
+        uint4 c = T[first * 32 + (i & 31)];
+        const uint4 d = __ldg(a.dtab + i);
+        c.x ^= d.x; c.y ^= d.y; c.z ^= d.z; c.w ^= d.w;
+        T[i] = c;
     }
-    return toff;
+    __syncthreads();
+}
+
+// D tables (see build_pass_tables) of every pass of one FFT: pass p's slot
+// 2^s - 1 + t holds the table of the value at offset t of heap layer
+// l0[p] + s, l0[p] = the layer of that pass's group roots.  One warp per
+// slot; blockIdx.y = pass.
+struct DtabArgs {
+    uint32_t l0[kMaxFftPasses], K[kMaxFftPasses];
+};
+__global__ void k_fft_dtab(const uint32_t *__restrict__ tw, DtabArgs d, uint32_t *__restrict__ out) {
+    const int lane = threadIdx.x & 31, p = blockIdx.y, K = (int)d.K[p];
+    const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (slot >= (1 << K) - 1) return;
+    const int s = 31 - __clz(slot + 1);
+    const uint64_t t = (uint64_t)(slot + 1 - (1 << s));
+    tab_build_warp(out + ((size_t)p * 63 + slot) * kTabWords, __ldg(tw + ((1ull << (d.l0[p] + s)) - 1) + t), lane);
 }
 
 // K stages over the NV values of a register pencil, node index of value i at
@@ -155,31 +181,35 @@ __device__ __forceinline__ void pencil_stages(uint32_t (&v)[1 << KP], const uint
 template <int K, bool INV>
 __global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
     extern __shared__ __align__(16) uint8_t smraw[];
+    // block -> (q, P, first chunk); the block walks the chunks of its
+    // (q, P) with stride a.nchunks, so its tables are built once
     const unsigned bid = blockIdx.x;
-    const unsigned chunk = bid & ((1u << a.log_bpg) - 1);
-    const unsigned rest = bid >> a.log_bpg;
+    const unsigned c0 = bid % a.nchunks;
+    const unsigned rest = bid / a.nchunks;
     const unsigned P = rest & ((1u << a.d0) - 1);
     const unsigned q = rest >> a.d0;
-    const uint32_t tb = build_pass_tables<K>(smraw, a, q, P);
-    __syncthreads();
+    build_pass_tables<K>(smraw, a, q, P);
+    const uint32_t tb = 0;
 
-    const uint64_t g = ((uint64_t)chunk << a.log_B) + threadIdx.x;
-    const uint64_t o = g & ((1ull << a.log_S) - 1);
-    const uint64_t j = g >> a.log_S;
-    if (j >= a.nvec) return;
-    uint32_t *base = a.data + j * a.col_stride + q * a.q_stride + ((uint64_t)P << (a.L - a.d0)) + o;
     const uint64_t S = 1ull << a.log_S;
-    uint32_t v[1 << K];
+    for (uint64_t chunk = c0; chunk < (1ull << a.log_bpg); chunk += a.nchunks) {
+        const uint64_t g = (chunk << a.log_B) + threadIdx.x;
+        const uint64_t o = g & ((1ull << a.log_S) - 1);
+        const uint64_t j = g >> a.log_S;
+        if (j >= a.nvec) break;
+        uint32_t *base = a.data + j * a.col_stride + q * a.q_stride + ((uint64_t)P << (a.L - a.d0)) + o;
+        uint32_t v[1 << K];
 #pragma unroll
-    for (int t = 0; t < (1 << K); ++t) v[t] = base[t * S];
-    pencil_stages<K, 0, INV>(v, smraw, tb, 0);
-    // recompute the store addresses instead of keeping 2^K pointers live
-    uint64_t S2;
-    asm volatile("mov.b64 %0, %1;" : "=l"(S2) : "l"(S));
-    uint32_t *base2;
-    asm volatile("mov.b64 %0, %1;" : "=l"(base2) : "l"(base));
+        for (int t = 0; t < (1 << K); ++t) v[t] = base[t * S];
+        pencil_stages<K, 0, INV>(v, smraw, tb, 0);
+        // recompute the store addresses instead of keeping 2^K pointers live
+        uint64_t S2;
+        asm volatile("mov.b64 %0, %1;" : "=l"(S2) : "l"(S));
+        uint32_t *base2;
+        asm volatile("mov.b64 %0, %1;" : "=l"(base2) : "l"(base));
 #pragma unroll
-    for (int t = 0; t < (1 << K); ++t) base2[t * S2] = v[t];
+        for (int t = 0; t < (1 << K); ++t) base2[t * S2] = v[t];
+    }
 }
 
 // Last pass (contiguous blocks of 2^K rows): one block per (q, P) tile of
@@ -198,7 +228,8 @@ __global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
     const unsigned P = rest & ((1u << a.d0) - 1);
     const unsigned q = rest >> a.d0;
     const uint32_t nvec = min(a.vchunk, a.nvec - chunk * a.vchunk);
-    const uint32_t tb = build_pass_tables<K>(smraw, a, q, P);
+    build_pass_tables<K>(smraw, a, q, P);
+    const uint32_t tb = 0;
     uint32_t *tile = reinterpret_cast<uint32_t *>(smraw + tb + ((1 << K) - 1) * 512);
     uint32_t *gbase = a.data + (uint64_t)chunk * a.vchunk * a.col_stride + q * a.q_stride + ((uint64_t)P << K);
 
@@ -210,10 +241,14 @@ __global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
     }
     __syncthreads();
 
+    // work items over (vector, piece) with the vector index in the low bits
+    // (a power-of-two span, so the split is a mask and a shift)
+    const uint32_t lnv = 32 - __clz(nvec - 1), vmask = (1u << lnv) - 1;
     auto phase_a = [&]() {
         if constexpr (KA > 0) {
-            for (uint32_t item = threadIdx.x; item < nvec * 16; item += blockDim.x) {
-                const uint32_t j = item % nvec, u = item / nvec;
+            for (uint32_t item = threadIdx.x; item < (16u << lnv); item += blockDim.x) {
+                const uint32_t j = item & vmask, u = item >> lnv;
+                if (j >= nvec) continue;
                 uint32_t v[1 << KA];
 #pragma unroll
                 for (int i = 0; i < (1 << KA); ++i) v[i] = tile[j * STRIDE + u + 16 * i];
@@ -224,8 +259,9 @@ __global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
         }
     };
     auto phase_b = [&]() {
-        for (uint32_t item = threadIdx.x; item < (nvec << KA); item += blockDim.x) {
-            const uint32_t j = item % nvec, gq = item / nvec;
+        for (uint32_t item = threadIdx.x; item < ((1u << KA) << lnv); item += blockDim.x) {
+            const uint32_t j = item & vmask, gq = item >> lnv;
+            if (j >= nvec) continue;
             uint32_t v[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) v[i] = tile[j * STRIDE + 16 * gq + i];
@@ -294,27 +330,40 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
 
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse, FftPasses passes) {
+                        uint32_t root_base, bool inverse) {
     if (log_len == 0 || nvec == 0) return cudaSuccess;
+    // the roots root_base + q (q < Q) must share one heap layer
+    const uint32_t lr = 31 - __builtin_clz(root_base);
+    if (!L.dtab || root_base == 0 || ((root_base + Q - 1) >> lr) != 1) return cudaErrorInvalidValue;
     // split log_len stages into passes of <= 6, balanced
     const uint32_t np = (log_len + 5) / 6;
+    if (np > kMaxFftPasses) return cudaErrorInvalidValue;
     std::vector<uint32_t> ks(np, log_len / np);
     for (uint32_t i = 0; i < log_len % np; ++i) ks[i] += 1;
     std::vector<uint32_t> d0s(np);
     for (uint32_t i = 0, d = 0; i < np; ++i) { d0s[i] = d; d += ks[i]; }
+    // D tables of every pass; kept while the same twiddle subtree is asked
+    // for again (the twiddle arrays live, unchanged, as long as the context)
+    const Launcher::DtabKey key{tw, log_len, root_base};
+    if (!(L.dtab_key == key)) {
+        DtabArgs d{};
+        for (uint32_t p = 0; p < np; ++p) { d.l0[p] = lr + d0s[p]; d.K[p] = ks[p]; }
+        LGK_LAUNCH(L, "fft_dtab", k_fft_dtab<<<dim3(8, np), 256, 0, L.stream>>>(tw, d, L.dtab));
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { L.dtab_key = {}; return e; }
+        L.dtab_key = key;
+    }
     uint32_t nvec_p2 = 1;
     while (nvec_p2 < nvec) nvec_p2 <<= 1;
     const bool aligned = ((uintptr_t)data % 16 == 0) && (col_stride % 4 == 0) && (q_stride % 4 == 0);
-    if (inverse && passes != FFT_ALL) return cudaErrorInvalidValue;
     for (uint32_t pi = 0; pi < np; ++pi) {
         const uint32_t p = inverse ? np - 1 - pi : pi;
-        if ((passes == FFT_HEAD && p == np - 1) || (passes == FFT_LAST && p != np - 1)) continue;
         const uint32_t K = ks[p], d0 = d0s[p];
         PassArgs a;
         a.data = data; a.tw = tw; a.col_stride = col_stride; a.q_stride = q_stride;
+        a.dtab = reinterpret_cast<const uint4 *>(L.dtab + (size_t)p * 63 * kTabWords);
         a.L = log_len; a.d0 = d0; a.log_S = log_len - d0 - K;
         a.log_nvec_p2 = ilog2u(nvec_p2); a.nvec = nvec; a.root_base = root_base;
-        a.vec_ok = aligned;
         const bool tail = a.log_S == 0 && K >= 4 && aligned;
         if (tail) {
             a.vchunk = std::min<uint32_t>(nvec, 64);
@@ -330,7 +379,10 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
         const uint32_t B = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>(G, 256));
         a.log_B = ilog2u(B);
         a.log_bpg = ilog2u(G / B);
-        const uint64_t blocks = ((uint64_t)Q << d0) << a.log_bpg;
+        // about 4 waves of resident blocks; each walks its chunks
+        const uint64_t groups = (uint64_t)Q << d0, bpg = 1ull << a.log_bpg;
+        a.nchunks = (uint32_t)std::min<uint64_t>(bpg, std::max<uint64_t>(1, (148ull * 8) / groups));
+        const uint64_t blocks = groups * a.nchunks;
         if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidValue;
         cudaError_t e = inverse ? launch_pass<true>(L, (int)K, a, (unsigned)blocks, B)
                                 : launch_pass<false>(L, (int)K, a, (unsigned)blocks, B);
@@ -364,6 +416,42 @@ __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint3
     uint4 *o = reinterpret_cast<uint4 *>(out + 8 * i);
     o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
     o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+}
+
+__global__ void k_leaf_block(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols, uint32_t b,
+                             uint32_t *__restrict__ out) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const uint32_t nb = (ncols + 15) / 16;
+    uint4 *o = reinterpret_cast<uint4 *>(out + 8 * i);
+    uint32_t cv[8];
+    if (b == 0) {
+        b3_iv(cv);
+    } else {
+        const uint4 x = o[0], y = o[1];
+        cv[0] = x.x; cv[1] = x.y; cv[2] = x.z; cv[3] = x.w;
+        cv[4] = y.x; cv[5] = y.y; cv[6] = y.z; cv[7] = y.w;
+    }
+    uint32_t m[16];
+#pragma unroll
+    for (int w = 0; w < 16; ++w) {
+        const uint32_t j = b * 16 + w;
+        m[w] = j < ncols ? __ldg(E + (uint64_t)j * rows + i) : 0u;
+    }
+    const bool last = b + 1 == nb;
+    const uint32_t blen = last ? 4 * ncols - 64 * (nb - 1) : 64;
+    const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
+    b3_compress(cv, m, blen, flags);
+    o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+    o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+}
+
+cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t b,
+                            uint32_t *out) {
+    if (ncols == 0 || ncols > 256 || b >= (ncols + 15) / 16) return cudaErrorInvalidValue;
+    const unsigned blocks = (unsigned)((rows + 127) / 128);
+    LGK_LAUNCH(L, "leaf_hash_block", k_leaf_block<<<blocks, 128, 0, L.stream>>>(E, rows, ncols, b, out));
+    return cudaGetLastError();
 }
 
 cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out) {
@@ -445,15 +533,17 @@ cudaError_t gather_rows(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t 
     return cudaGetLastError();
 }
 __global__ void k_gather_nodes(const uint32_t *__restrict__ tree, const uint64_t *__restrict__ idx,
-                               uint32_t count, uint32_t *__restrict__ out) {
+                               uint32_t count, const uint32_t *d_count, uint32_t *__restrict__ out) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d_count) count = min(count, *d_count);
     if (t >= count * 8) return;
     out[t] = tree[8 * idx[t / 8] + (t % 8)];
 }
 cudaError_t gather_nodes(Launcher &L, const uint32_t *tree, const uint64_t *d_node_index, uint32_t count,
-                         uint32_t *out) {
+                         uint32_t *out, const uint32_t *d_count) {
     if (count == 0) return cudaSuccess;
-    LGK_LAUNCH(L, "gather_nodes", k_gather_nodes<<<(count * 8 + 255) / 256, 256, 0, L.stream>>>(tree, d_node_index, count, out));
+    LGK_LAUNCH(L, "gather_nodes",
+               k_gather_nodes<<<(count * 8 + 255) / 256, 256, 0, L.stream>>>(tree, d_node_index, count, d_count, out));
     return cudaGetLastError();
 }
 
@@ -462,12 +552,24 @@ struct Coeffs64 { uint32_t v[64]; };
 
 // partial_eval over k top variables at once: out[i] = sum_j gr[j] in[j*M+i]
 // with gr the Lagrange (eq) basis of the k challenges; one table per gr[j].
+// evaluate_lagrange_basis (src/utils.rs:4-27) entry j of k challenges:
+// rs[0] selects the index MSB, factor rs[i] where the bit is set, 1 + rs[i]
+// where not (field products commute, so the order is immaterial).
+__device__ __forceinline__ uint32_t lagrange_at(const uint32_t *rs, uint32_t k, uint32_t j) {
+    uint32_t p = 1;
+    for (uint32_t i = 0; i < k; ++i) p = gf_mul(p, ((j >> (k - 1 - i)) & 1) ? rs[i] : 1u ^ rs[i]);
+    return p;
+}
+
 __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-                                                 uint64_t M, uint32_t nj, Coeffs64 gr) {
+                                                 uint64_t M, uint32_t nj, Coeffs64 gr, const uint32_t *d_rs,
+                                                 uint32_t k) {
     extern __shared__ __align__(128) uint8_t tabs8[];
+    __shared__ uint32_t g[64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (uint32_t j = warp; j < nj; j += nw)
-        tab_build_warp(reinterpret_cast<uint32_t *>(tabs8 + 512 * j), gr.v[j], lane);
+    if (threadIdx.x < nj) g[threadIdx.x] = d_rs ? lagrange_at(d_rs, k, threadIdx.x) : gr.v[threadIdx.x];
+    __syncthreads();
+    for (uint32_t j = warp; j < nj; j += nw) tab_build_warp(reinterpret_cast<uint32_t *>(tabs8 + 512 * j), g[j], lane);
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t acc = 0;
@@ -477,14 +579,15 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
 }
 
 cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
-                    const uint32_t *gr) {
-    if (k < 1 || k > 6 || k > log_len) return cudaErrorInvalidValue;
+                    const uint32_t *gr, const uint32_t *d_rs) {
+    if (k < 1 || k > 6 || k > log_len || (!gr && !d_rs)) return cudaErrorInvalidValue;
     Coeffs64 c{};
     const uint32_t nj = 1u << k;
-    for (uint32_t j = 0; j < nj; ++j) c.v[j] = gr[j];
+    if (!d_rs)
+        for (uint32_t j = 0; j < nj; ++j) c.v[j] = gr[j];
     const uint64_t M = 1ull << (log_len - k);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((M + 255) / 256, 148ull * 8));
-    LGK_LAUNCH(L, "fold_eq", k_fold_eq<<<blocks, 256, nj * kTabWords * sizeof(uint32_t), L.stream>>>(in, out, M, nj, c));
+    LGK_LAUNCH(L, "fold_eq", k_fold_eq<<<blocks, 256, nj * kTabWords * sizeof(uint32_t), L.stream>>>(in, out, M, nj, c, d_rs, k));
     return cudaGetLastError();
 }
 
@@ -510,7 +613,7 @@ __device__ __forceinline__ uint32_t at3(uint32_t lo, uint32_t hi) { return gf_mu
 
 // eval_013_product (src/multilinear_poly.rs:90-131)
 __global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__restrict__ g, uint64_t half,
-                          uint32_t *acc3) {
+                          uint32_t *acc3, FsTail tail) {
     uint32_t s0 = 0, s1 = 0, s2 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t f0 = f[i], f1 = f[half + i], g0 = g[i], g1 = g[half + i];
@@ -519,11 +622,14 @@ __global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__rest
         s2 ^= gf_mul(at3(f0, f1), at3(g0, g1));
     }
     block_xor3(s0, s1, s2, acc3);
+    if (tail.fs) fsd::fs_tail_block(tail, acc3);
 }
-cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t log_len, uint32_t *acc3) {
+cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t log_len, uint32_t *acc3,
+                    const FsTail *tail) {
     const uint64_t half = 1ull << (log_len - 1);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((half + 255) / 256, 148ull * 4));
-    LGK_LAUNCH(L, "eval013", k_eval013<<<blocks, 256, 0, L.stream>>>(f, g, half, acc3));
+    const FsTail t = tail ? *tail : FsTail{};
+    LGK_LAUNCH(L, "eval013", k_eval013<<<blocks, 256, 0, L.stream>>>(f, g, half, acc3, t));
     return cudaGetLastError();
 }
 
@@ -531,10 +637,11 @@ cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t 
 // and of the (summed) basis by r, (1+r)a + r b = a + r(a+b), then
 // eval_01x_product on the folded pair.
 __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__ f, const uint32_t *__restrict__ B,
-                                                    uint64_t quarter, uint32_t r, uint32_t *__restrict__ fo,
-                                                    uint32_t *__restrict__ Bo, uint32_t *acc3) {
+                                                    uint64_t quarter, uint32_t r, const uint32_t *d_r,
+                                                    uint32_t *__restrict__ fo, uint32_t *__restrict__ Bo,
+                                                    uint32_t *acc3, FsTail tail) {
     __shared__ __align__(128) uint32_t T[kTabWords];
-    if (threadIdx.x < 32) tab_build_warp(T, r, threadIdx.x);
+    if (threadIdx.x < 32) tab_build_warp(T, d_r ? *d_r : r, threadIdx.x);
     __syncthreads();
     const uint8_t *t8 = reinterpret_cast<const uint8_t *>(T);
     uint32_t s0 = 0, s1 = 0, s2 = 0;
@@ -550,28 +657,32 @@ __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__
         s2 ^= gf_mul(at3(flo, fhi), at3(blo, bhi));
     }
     block_xor3(s0, s1, s2, acc3);
+    if (tail.fs) fsd::fs_tail_block(tail, acc3);
 }
 cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32_t log_len, uint32_t r,
-                       uint32_t *fo, uint32_t *Bo, uint32_t *acc3) {
+                       uint32_t *fo, uint32_t *Bo, uint32_t *acc3, const uint32_t *d_r, const FsTail *tail) {
     if (log_len < 2) return cudaErrorInvalidValue;
     const uint64_t quarter = 1ull << (log_len - 2);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((quarter + 255) / 256, 148ull * 4));
-    LGK_LAUNCH(L, "fold_round", k_fold_round<<<blocks, 256, 0, L.stream>>>(f, B, quarter, r, fo, Bo, acc3));
+    LGK_LAUNCH(L, "fold_round", k_fold_round<<<blocks, 256, 0, L.stream>>>(f, B, quarter, r, d_r, fo, Bo, acc3,
+                                                                                tail ? *tail : FsTail{}));
     return cudaGetLastError();
 }
 
 // glue (src/ligerito.rs:59-67) folded into the running basis sum
-__global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi, uint64_t n, uint32_t beta) {
+__global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi, uint64_t n, uint32_t beta,
+                       const uint32_t *d_beta) {
     __shared__ __align__(128) uint32_t T[kTabWords];
-    if (threadIdx.x < 32) tab_build_warp(T, beta, threadIdx.x);
+    if (threadIdx.x < 32) tab_build_warp(T, d_beta ? *d_beta : beta, threadIdx.x);
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         B[i] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(T), 0, 0, bi[i]);
 }
-cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta) {
+cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta,
+                 const uint32_t *d_beta) {
     const uint64_t n = 1ull << log_len;
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 4));
-    LGK_LAUNCH(L, "axpy", k_axpy<<<blocks, 256, 0, L.stream>>>(B, bi, n, beta));
+    LGK_LAUNCH(L, "axpy", k_axpy<<<blocks, 256, 0, L.stream>>>(B, bi, n, beta, d_beta));
     return cudaGetLastError();
 }
 
@@ -605,11 +716,17 @@ struct InduceSetupArgs {
 };
 __global__ void k_induce_setup(const uint32_t *__restrict__ rows, uint32_t glen, const uint64_t *__restrict__ q,
                                uint32_t nq, uint32_t alpha, uint32_t n, InduceSetupArgs args,
-                               uint32_t *__restrict__ S, uint32_t *__restrict__ apow, uint32_t *sum_out) {
+                               uint32_t *__restrict__ S, uint32_t *__restrict__ apow, uint32_t *sum_out,
+                               const uint32_t *d_rs, uint32_t nch, const uint32_t *d_alpha) {
+    // gr: the Lagrange basis of the challenges (from the device when given)
+    __shared__ uint32_t gr[256];
+    for (uint32_t j = threadIdx.x; j < glen; j += blockDim.x) gr[j] = d_rs ? lagrange_at(d_rs, nch, j) : args.gr[j];
+    if (d_alpha) alpha = *d_alpha;
+    __syncthreads();
     uint32_t contrib = 0;
     for (uint32_t k = threadIdx.x; k < nq; k += blockDim.x) {
         uint32_t dot = 0;
-        for (uint32_t j = 0; j < glen; ++j) dot ^= gf_mul(rows[(uint64_t)k * glen + j], args.gr[j]);
+        for (uint32_t j = 0; j < glen; ++j) dot ^= gf_mul(rows[(uint64_t)k * glen + j], gr[j]);
         uint32_t p = 1, base = alpha;
         for (uint32_t e = k; e; e >>= 1) {
             if (e & 1) p = gf_mul(p, base);
@@ -637,14 +754,17 @@ __global__ void k_induce_setup(const uint32_t *__restrict__ rows, uint32_t glen,
 
 cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
                          const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
-                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum) {
-    if (glen > 256 || n > 32 || nq == 0) return cudaErrorInvalidValue;
+                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum, const uint32_t *d_rs,
+                         const uint32_t *d_alpha) {
+    if (glen > 256 || n > 32 || nq == 0 || (glen & (glen - 1)) || (!gr && !d_rs)) return cudaErrorInvalidValue;
     InduceSetupArgs args{};
-    for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
+    if (!d_rs)
+        for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
     for (uint32_t i = 0; i + 1 < n && i < 32; ++i) args.sks[i] = sks[i];
     const unsigned threads = std::min<unsigned>(256, ((nq + 31) / 32) * 32);
     LGK_LAUNCH(L, "induce_setup", k_induce_setup<<<1, threads, 0, L.stream>>>(d_rows, glen, d_q, nq, alpha, n, args,
-                                                                           d_S, d_apow, d_sum));
+                                                                           d_S, d_apow, d_sum, d_rs,
+                                                                           ilog2u(glen), d_alpha));
     return cudaGetLastError();
 }
 

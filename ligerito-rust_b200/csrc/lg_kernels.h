@@ -12,8 +12,22 @@ namespace lgk {
 
 // Counts every kernel launch and, when timing is on, brackets each with a
 // pair of CUDA events on the launching stream (resolved lazily).
+// An FFT of up to 2^30 points runs in at most 5 passes of <= 6 stages; a
+// pass has at most 63 node tables of 128 words.
+constexpr uint32_t kMaxFftPasses = 5;
+constexpr size_t kDtabWords = kMaxFftPasses * 63 * 128;
+
 struct Launcher {
     cudaStream_t stream = nullptr;
+    // device scratch of kDtabWords, owned by the context: the FFT passes'
+    // shared twiddle tables (fft_vectors), reused in stream order, and the
+    // twiddle subtree they were built for
+    uint32_t *dtab = nullptr;
+    struct DtabKey {
+        const uint32_t *tw = nullptr;
+        uint32_t log_len = 0, root_base = 0;
+        bool operator==(const DtabKey &o) const { return tw == o.tw && log_len == o.log_len && root_base == o.root_base; }
+    } dtab_key;
     uint64_t launches = 0;
     bool timing = false;
     struct Pending { std::string name; cudaEvent_t a, b; };
@@ -28,6 +42,15 @@ struct Launcher {
     void release();
 };
 
+// A kernel launch on L's stream, counted and (when timing) bracketed.
+#define LGK_LAUNCH(L, name, ...)   \
+    do {                           \
+        cudaEvent_t _ev = nullptr; \
+        (L).begin(name, &_ev);     \
+        __VA_ARGS__;               \
+        (L).end(name, _ev);        \
+    } while (0)
+
 // --- Reed-Solomon column encoding (src/reed_solomon.rs:104-113) ----------
 // E (column-major, n columns of 4m): every quarter of column j receives
 // poly[j*m + i] * pis[i]; the zero-padded 4m-point FFT's top two stages are
@@ -39,40 +62,51 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
 // vectors of 2^log_len: vector (j, q) starts at data + j*col_stride +
 // q*q_stride and uses the twiddle subtree under heap node root_base + q of
 // `tw` (heap order, tw[idx-1]).
-// passes: FFT_ALL, FFT_HEAD (every pass but the last), FFT_LAST (only the
-// last; forward only) -- the head passes treat vectors independently, so a
-// batch may run them in column groups and the last pass once for all.
-enum FftPasses { FFT_ALL = 0, FFT_HEAD = 1, FFT_LAST = 2 };
+// The twiddle arrays must stay allocated and unchanged for the Launcher's
+// lifetime (its cached pass tables are keyed by their address).
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse, FftPasses passes = FFT_ALL);
+                        uint32_t root_base, bool inverse);
 
 // --- Merkle (src/merkle_tree.rs:4-60, leaves src/ligero.rs:53-68) --------
 // Leaf hash of every row of a column-major matrix (rows x ncols u32).
 cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out);
+// BLAKE3 block b (columns 16b .. 16b+15) of every leaf: chains from the
+// value in out (the IV for b = 0) and leaves the chaining value there, the
+// leaf hash after the last block.  Blocks run in order 0, 1, ...
+cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t b,
+                            uint32_t *out);
 // All upper layers from the leaf layer at tree[0]; tree as 8-word nodes.
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves);
 
 // --- gathers for openings (src/ligero.rs:40-51, src/merkle_tree.rs:98) ---
 cudaError_t gather_rows(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols,
                         const uint64_t *d_queries, uint32_t nq, uint32_t *out);
+// count nodes, or min(count, *d_count) when d_count is given
 cudaError_t gather_nodes(Launcher &L, const uint32_t *tree, const uint64_t *d_node_index,
-                         uint32_t count, uint32_t *out);
+                         uint32_t count, uint32_t *out, const uint32_t *d_count = nullptr);
 
 // --- multilinear folds (src/multilinear_poly.rs:66-87) -------------------
-// out[i] = sum_j gr[j] * in[j*M + i], M = 2^log_len >> k, 1 <= k <= 6.
+// out[i] = sum_j gr[j] * in[j*M + i], M = 2^log_len >> k, 1 <= k <= 6;
+// gr given on the host, or the Lagrange basis of the k device challenges
+// d_rs.
 cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
-                    const uint32_t *gr);
+                    const uint32_t *gr, const uint32_t *d_rs = nullptr);
+
+struct FsTail;  // a fused transcript step, below
 
 // --- sumcheck rounds (src/ligerito.rs:50-127, multilinear_poly.rs:90) -----
 // acc3 (device, 3 words) is XOR-accumulated; the caller zeroes it.
 cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t log_len,
-                    uint32_t *acc3);
-// f, B of 2^log_len folded by r into fo, Bo (2^(log_len-1)); triple of (fo, Bo)
+                    uint32_t *acc3, const FsTail *tail = nullptr);
+// f, B of 2^log_len folded by r (or *d_r) into fo, Bo (2^(log_len-1));
+// triple of (fo, Bo)
 cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32_t log_len,
-                       uint32_t r, uint32_t *fo, uint32_t *Bo, uint32_t *acc3);
-// B ^= beta * bi
-cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta);
+                       uint32_t r, uint32_t *fo, uint32_t *Bo, uint32_t *acc3, const uint32_t *d_r = nullptr,
+                       const FsTail *tail = nullptr);
+// B ^= beta * bi (beta or *d_beta)
+cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta,
+                 const uint32_t *d_beta = nullptr);
 
 // --- induce_sumcheck_poly basis (src/sumcheck_polys.rs:74-160) ------------
 // basis[t] = sum_k apow[k] * prod_{bit i of t} S[k*n + i]; S = per-query
@@ -85,11 +119,73 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
                          uint32_t *out);
 
 // Per-query inputs of induce_basis from device-resident opened rows
-// (nq x glen): S (nq x n), apow (nq) and the enforced sum (1 word).
+// (nq x glen): S (nq x n), apow (nq) and the enforced sum (1 word).  gr
+// and alpha from the host, or the Lagrange basis of log2(glen) device
+// challenges d_rs and *d_alpha.
 cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
                          const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
-                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum);
+                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum, const uint32_t *d_rs = nullptr,
+                         const uint32_t *d_alpha = nullptr);
 
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);
+
+// --- Fiat-Shamir transcript on the device (src/emulated_fs.rs:6-76) ------
+// The running SHA-256 of the transcript: the host's lg::Transcript with the
+// pending bytes kept as big-endian words (the transcript only ever absorbs
+// whole u32s and 32-byte roots, so they stay word-aligned).
+struct FsState {
+    uint32_t h[8];
+    uint32_t w[16];    // pending message words
+    uint64_t total;    // bytes absorbed
+    uint32_t nw;       // words pending in w
+    uint32_t counter;  // squeezes so far
+    uint32_t err;      // FS_ERR_* bits: a prover assertion failed
+    uint32_t pad;
+};
+enum : uint32_t { FS_ERR_SUMCHECK = 1, FS_ERR_QUERIES = 2 };
+
+// A transcript step fused into a sumcheck kernel (eval013, fold_round): its
+// last block to finish absorbs the kernel's triple -- asserting first, when
+// check is set, that triple[0] ^ triple[1] == triple[3] (the enforced sum)
+// -- and squeezes nsq field elements into out.  ticket: a zeroed word the
+// kernel counts finished blocks in (left zero again).
+struct FsTail {
+    FsState *fs = nullptr;
+    uint32_t *ticket = nullptr;
+    uint32_t check = 0;
+    uint32_t nsq = 0;
+    uint32_t *out = nullptr;
+};
+
+// FS::new(seed)
+cudaError_t fs_init(Launcher &L, FsState *d, uint32_t seed);
+// If check: flag FS_ERR_SUMCHECK unless src[0] ^ src[1] == src[3] (a
+// sumcheck triple and its enforced sum).  Then absorb nwords u32s of src
+// (their LE bytes) and squeeze nsq field elements into out.
+struct FsStep {
+    const uint32_t *src = nullptr;
+    uint32_t nwords = 0, check = 0;
+    uint32_t nsq = 0;
+    uint32_t *out = nullptr;
+};
+cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a);
+// Absorb nwords u32s of src; get_distinct_queries(n, s) sorted into q
+// (s <= 256, n a power of two); the multi-proof siblings of those leaves
+// in a tree of n leaves (merkle_tree::prove order) into nodes as node
+// numbers, leaves first, count in *nnodes; then squeeze nsq field elements
+// into out.  n < s flags FS_ERR_QUERIES (the reference loops forever).
+struct FsQueries {
+    const uint32_t *src = nullptr;
+    uint32_t nwords = 0;
+    uint64_t n = 0;
+    uint32_t s = 0;
+    uint64_t *q = nullptr;
+    uint64_t *nodes = nullptr;
+    uint32_t nodes_cap = 0;
+    uint32_t *nnodes = nullptr;
+    uint32_t nsq = 0;
+    uint32_t *out = nullptr;
+};
+cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a);
 
 }  // namespace lgk
