@@ -18,6 +18,15 @@
 
 namespace lgd {
 
+// Programmatic dependent launch: wait until the previous grid on the
+// stream has completed and its writes are visible, then let the next grid
+// start launching (its blocks in turn wait here).  A no-op for launches
+// without the attribute.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 constexpr uint32_t kTail = 0x8299u;  // x^32 mod p
 
 __device__ __forceinline__ uint32_t red_small(uint32_t t) {

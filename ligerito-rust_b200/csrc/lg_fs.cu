@@ -16,6 +16,7 @@
 // part), then every thread finalises its own clone in parallel.
 #include <cstdint>
 
+#include "lg_device.cuh"
 #include "lg_fs.cuh"
 
 namespace lgk {
@@ -23,8 +24,10 @@ namespace lgk {
 namespace {
 
 using namespace fsd;
+using lgd::pdl_begin;
 
 __global__ void k_fs_init(FsState *g, uint32_t seed) {
+    pdl_begin();
     __shared__ FsState S;
     if (threadIdx.x == 0) {
         const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
@@ -41,6 +44,7 @@ __global__ void k_fs_init(FsState *g, uint32_t seed) {
 }
 
 __global__ void k_fs_step(FsState *g, FsStep a) {
+    pdl_begin();
     __shared__ FsState S;
     __shared__ Batch B;
     load_state(S, g);
@@ -72,6 +76,7 @@ __device__ uint32_t block_rank(bool flag, uint32_t *scratch, uint32_t *total) {
 }
 
 __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a) {
+    pdl_begin();
     __shared__ FsState S;
     __shared__ Batch B;
     __shared__ uint64_t acc[kQBlock], cand[kQBlock];
@@ -192,20 +197,20 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a)
 }  // namespace
 
 cudaError_t fs_init(Launcher &L, FsState *d, uint32_t seed) {
-    LGK_LAUNCH(L, "fs_init", k_fs_init<<<1, 32, 0, L.stream>>>(d, seed));
+    LGK_LAUNCH(L, "fs_init", launch_k(k_fs_init, 1, 32, 0, L.stream, d, seed));
     return cudaGetLastError();
 }
 
 cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a) {
     if (a.nwords > 1024 || a.nsq > 256 || (a.check && (!a.src || a.nwords < 3))) return cudaErrorInvalidValue;
-    LGK_LAUNCH(L, "fs_step", k_fs_step<<<1, 32, 0, L.stream>>>(d, a));
+    LGK_LAUNCH(L, "fs_step", launch_k(k_fs_step, 1, 32, 0, L.stream, d, a));
     return cudaGetLastError();
 }
 
 cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a) {
     if (a.s == 0 || a.s > kQBlock || a.n == 0 || (a.n & (a.n - 1)) || a.nwords > 1024 || a.nsq > kQBlock)
         return cudaErrorInvalidValue;
-    LGK_LAUNCH(L, "fs_queries", k_fs_queries<<<1, kQBlock, 0, L.stream>>>(d, a));
+    LGK_LAUNCH(L, "fs_queries", launch_k(k_fs_queries, 1, kQBlock, 0, L.stream, d, a));
     return cudaGetLastError();
 }
 

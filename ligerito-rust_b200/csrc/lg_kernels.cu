@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 using namespace lgd;
 
@@ -55,11 +56,20 @@ void Launcher::release() {
 }
 
 
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("LG_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 static inline unsigned ilog2u(uint64_t x) { unsigned r = 0; while (x > 1) { x >>= 1; ++r; } return r; }
 
 // ====================================================== RS scale + spread
 __global__ void k_rs_scale_spread(const uint32_t *__restrict__ poly, const uint32_t *__restrict__ pis,
                                   uint32_t *__restrict__ E, uint32_t log_m, uint64_t total) {
+    pdl_begin();
     const uint64_t m = 1ull << log_m;
     for (uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; idx < total;
          idx += (uint64_t)gridDim.x * blockDim.x) {
@@ -77,7 +87,7 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
                             uint32_t log_m, uint32_t n) {
     uint64_t total = (uint64_t)n << log_m;
     unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
-    LGK_LAUNCH(L, "rs_scale_spread", k_rs_scale_spread<<<blocks, 256, 0, L.stream>>>(poly, pis, E, log_m, total));
+    LGK_LAUNCH(L, "rs_scale_spread", launch_k(k_rs_scale_spread, blocks, 256, 0, L.stream, poly, pis, E, log_m, total));
     return cudaGetLastError();
 }
 
@@ -135,6 +145,7 @@ struct DtabArgs {
     uint32_t l0[kMaxFftPasses], K[kMaxFftPasses];
 };
 __global__ void k_fft_dtab(const uint32_t *__restrict__ tw, DtabArgs d, uint32_t *__restrict__ out) {
+    pdl_begin();
     const int lane = threadIdx.x & 31, p = blockIdx.y, K = (int)d.K[p];
     const int slot = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (slot >= (1 << K) - 1) return;
@@ -180,6 +191,7 @@ __device__ __forceinline__ void pencil_stages(uint32_t (&v)[1 << KP], const uint
 // the pass; lanes run over o, so each row access is coalesced.
 template <int K, bool INV>
 __global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
+    pdl_begin();
     extern __shared__ __align__(16) uint8_t smraw[];
     // block -> (q, P, first chunk); the block walks the chunks of its
     // (q, P) with stride a.nchunks, so its tables are built once
@@ -222,6 +234,7 @@ __global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
 // over vectors, so a warp shares every table it reads.
 template <int K, bool INV>
 __global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
+    pdl_begin();
     constexpr int KA = K - 4, R = 1 << K, STRIDE = R + 1, CPC = R / 4;
     extern __shared__ __align__(16) uint8_t smraw[];
     const unsigned chunk = blockIdx.x % a.nchunks, rest = blockIdx.x / a.nchunks;
@@ -301,7 +314,7 @@ static cudaError_t launch_pass(Launcher &L, int K, PassArgs a, unsigned blocks, 
     case k:                                                                                          \
         if (smem > 48 * 1024)                                                                        \
             cudaFuncSetAttribute(k_fft_pass<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        LGK_LAUNCH(L, nmbuf, k_fft_pass<k, INV><<<blocks, threads, smem, L.stream>>>(a));            \
+        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_pass<k, INV>, blocks, threads, smem, L.stream, a));            \
         break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
@@ -319,7 +332,7 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
 #define LGK_CASE(k)                                                                                 \
     case k:                                                                                         \
         cudaFuncSetAttribute(k_fft_tail<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        LGK_LAUNCH(L, nmbuf, k_fft_tail<k, INV><<<blocks, 256, smem, L.stream>>>(a));               \
+        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_tail<k, INV>, blocks, 256, smem, L.stream, a));               \
         break;
         LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
@@ -348,7 +361,7 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
     if (!(L.dtab_key == key)) {
         DtabArgs d{};
         for (uint32_t p = 0; p < np; ++p) { d.l0[p] = lr + d0s[p]; d.K[p] = ks[p]; }
-        LGK_LAUNCH(L, "fft_dtab", k_fft_dtab<<<dim3(8, np), 256, 0, L.stream>>>(tw, d, L.dtab));
+        LGK_LAUNCH(L, "fft_dtab", launch_k(k_fft_dtab, dim3(8, np), 256, 0, L.stream, tw, d, L.dtab));
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { L.dtab_key = {}; return e; }
         L.dtab_key = key;
@@ -396,6 +409,7 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
 // blocks of 16 words, CHUNK_START on the first, CHUNK_END|ROOT on the last.
 __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
                             uint32_t *__restrict__ out) {
+    pdl_begin();
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const uint32_t nb = (ncols + 15) / 16;
@@ -420,6 +434,7 @@ __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint3
 
 __global__ void k_leaf_block(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols, uint32_t b,
                              uint32_t *__restrict__ out) {
+    pdl_begin();
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const uint32_t nb = (ncols + 15) / 16;
@@ -450,13 +465,13 @@ cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint3
                             uint32_t *out) {
     if (ncols == 0 || ncols > 256 || b >= (ncols + 15) / 16) return cudaErrorInvalidValue;
     const unsigned blocks = (unsigned)((rows + 127) / 128);
-    LGK_LAUNCH(L, "leaf_hash_block", k_leaf_block<<<blocks, 128, 0, L.stream>>>(E, rows, ncols, b, out));
+    LGK_LAUNCH(L, "leaf_hash_block", launch_k(k_leaf_block, blocks, 128, 0, L.stream, E, rows, ncols, b, out));
     return cudaGetLastError();
 }
 
 cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out) {
     const unsigned blocks = (unsigned)((rows + 127) / 128);
-    LGK_LAUNCH(L, "leaf_hash", k_leaf_hash<<<blocks, 128, 0, L.stream>>>(E, rows, ncols, out));
+    LGK_LAUNCH(L, "leaf_hash", launch_k(k_leaf_hash, blocks, 128, 0, L.stream, E, rows, ncols, out));
     return cudaGetLastError();
 }
 
@@ -475,6 +490,7 @@ __device__ __forceinline__ void hash_node(const uint32_t *l, const uint32_t *r, 
 }
 
 __global__ void k_merkle_sub(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in, uint32_t c) {
+    pdl_begin();
     extern __shared__ uint32_t sm[];  // 2 * 2^c * 8 words
     const uint32_t width = 1u << c;
     uint32_t *cur = sm, *nxt = sm + 8 * width;
@@ -510,7 +526,7 @@ cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
         const unsigned blocks = (unsigned)(n / width);
         const unsigned threads = std::max<unsigned>(32, std::min<unsigned>(width / 2, 128));
         const size_t smem = 2ull * width * 8 * sizeof(uint32_t);
-        LGK_LAUNCH(L, "merkle_layers", k_merkle_sub<<<blocks, threads, smem, L.stream>>>(tree, off, n, c));
+        LGK_LAUNCH(L, "merkle_layers", launch_k(k_merkle_sub, blocks, threads, smem, L.stream, tree, off, n, c));
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         for (uint32_t l = 0; l < c; ++l) { off += n; n /= 2; }
@@ -521,6 +537,7 @@ cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
 // ============================================================== gathers
 __global__ void k_gather_rows(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
                               const uint64_t *__restrict__ q, uint32_t nq, uint32_t *__restrict__ out) {
+    pdl_begin();
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= nq * ncols) return;
     const uint32_t k = idx / ncols, j = idx % ncols;
@@ -529,11 +546,12 @@ __global__ void k_gather_rows(const uint32_t *__restrict__ E, uint64_t rows, uin
 cudaError_t gather_rows(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols,
                         const uint64_t *d_queries, uint32_t nq, uint32_t *out) {
     const uint32_t total = nq * ncols;
-    LGK_LAUNCH(L, "gather_rows", k_gather_rows<<<(total + 255) / 256, 256, 0, L.stream>>>(E, rows, ncols, d_queries, nq, out));
+    LGK_LAUNCH(L, "gather_rows", launch_k(k_gather_rows, (total + 255) / 256, 256, 0, L.stream, E, rows, ncols, d_queries, nq, out));
     return cudaGetLastError();
 }
 __global__ void k_gather_nodes(const uint32_t *__restrict__ tree, const uint64_t *__restrict__ idx,
                                uint32_t count, const uint32_t *d_count, uint32_t *__restrict__ out) {
+    pdl_begin();
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (d_count) count = min(count, *d_count);
     if (t >= count * 8) return;
@@ -543,7 +561,7 @@ cudaError_t gather_nodes(Launcher &L, const uint32_t *tree, const uint64_t *d_no
                          uint32_t *out, const uint32_t *d_count) {
     if (count == 0) return cudaSuccess;
     LGK_LAUNCH(L, "gather_nodes",
-               k_gather_nodes<<<(count * 8 + 255) / 256, 256, 0, L.stream>>>(tree, d_node_index, count, d_count, out));
+               launch_k(k_gather_nodes, (count * 8 + 255) / 256, 256, 0, L.stream, tree, d_node_index, count, d_count, out));
     return cudaGetLastError();
 }
 
@@ -564,6 +582,7 @@ __device__ __forceinline__ uint32_t lagrange_at(const uint32_t *rs, uint32_t k, 
 __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
                                                  uint64_t M, uint32_t nj, Coeffs64 gr, const uint32_t *d_rs,
                                                  uint32_t k) {
+    pdl_begin();
     extern __shared__ __align__(128) uint8_t tabs8[];
     __shared__ uint32_t g[64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -587,7 +606,7 @@ cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log
         for (uint32_t j = 0; j < nj; ++j) c.v[j] = gr[j];
     const uint64_t M = 1ull << (log_len - k);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((M + 255) / 256, 148ull * 8));
-    LGK_LAUNCH(L, "fold_eq", k_fold_eq<<<blocks, 256, nj * kTabWords * sizeof(uint32_t), L.stream>>>(in, out, M, nj, c, d_rs, k));
+    LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq, blocks, 256, nj * kTabWords * sizeof(uint32_t), L.stream, in, out, M, nj, c, d_rs, k));
     return cudaGetLastError();
 }
 
@@ -614,6 +633,7 @@ __device__ __forceinline__ uint32_t at3(uint32_t lo, uint32_t hi) { return gf_mu
 // eval_013_product (src/multilinear_poly.rs:90-131)
 __global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__restrict__ g, uint64_t half,
                           uint32_t *acc3, FsTail tail) {
+    pdl_begin();
     uint32_t s0 = 0, s1 = 0, s2 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t f0 = f[i], f1 = f[half + i], g0 = g[i], g1 = g[half + i];
@@ -629,7 +649,7 @@ cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t 
     const uint64_t half = 1ull << (log_len - 1);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((half + 255) / 256, 148ull * 4));
     const FsTail t = tail ? *tail : FsTail{};
-    LGK_LAUNCH(L, "eval013", k_eval013<<<blocks, 256, 0, L.stream>>>(f, g, half, acc3, t));
+    LGK_LAUNCH(L, "eval013", launch_k(k_eval013, blocks, 256, 0, L.stream, f, g, half, acc3, t));
     return cudaGetLastError();
 }
 
@@ -640,6 +660,7 @@ __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__
                                                     uint64_t quarter, uint32_t r, const uint32_t *d_r,
                                                     uint32_t *__restrict__ fo, uint32_t *__restrict__ Bo,
                                                     uint32_t *acc3, FsTail tail) {
+    pdl_begin();
     __shared__ __align__(128) uint32_t T[kTabWords];
     if (threadIdx.x < 32) tab_build_warp(T, d_r ? *d_r : r, threadIdx.x);
     __syncthreads();
@@ -664,7 +685,7 @@ cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32
     if (log_len < 2) return cudaErrorInvalidValue;
     const uint64_t quarter = 1ull << (log_len - 2);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((quarter + 255) / 256, 148ull * 4));
-    LGK_LAUNCH(L, "fold_round", k_fold_round<<<blocks, 256, 0, L.stream>>>(f, B, quarter, r, d_r, fo, Bo, acc3,
+    LGK_LAUNCH(L, "fold_round", launch_k(k_fold_round, blocks, 256, 0, L.stream, f, B, quarter, r, d_r, fo, Bo, acc3,
                                                                                 tail ? *tail : FsTail{}));
     return cudaGetLastError();
 }
@@ -672,6 +693,7 @@ cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32
 // glue (src/ligerito.rs:59-67) folded into the running basis sum
 __global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi, uint64_t n, uint32_t beta,
                        const uint32_t *d_beta) {
+    pdl_begin();
     __shared__ __align__(128) uint32_t T[kTabWords];
     if (threadIdx.x < 32) tab_build_warp(T, d_beta ? *d_beta : beta, threadIdx.x);
     __syncthreads();
@@ -682,7 +704,7 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
                  const uint32_t *d_beta) {
     const uint64_t n = 1ull << log_len;
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 4));
-    LGK_LAUNCH(L, "axpy", k_axpy<<<blocks, 256, 0, L.stream>>>(B, bi, n, beta, d_beta));
+    LGK_LAUNCH(L, "axpy", launch_k(k_axpy, blocks, 256, 0, L.stream, B, bi, n, beta, d_beta));
     return cudaGetLastError();
 }
 
@@ -718,6 +740,7 @@ __global__ void k_induce_setup(const uint32_t *__restrict__ rows, uint32_t glen,
                                uint32_t nq, uint32_t alpha, uint32_t n, InduceSetupArgs args,
                                uint32_t *__restrict__ S, uint32_t *__restrict__ apow, uint32_t *sum_out,
                                const uint32_t *d_rs, uint32_t nch, const uint32_t *d_alpha) {
+    pdl_begin();
     // gr: the Lagrange basis of the challenges (from the device when given)
     __shared__ uint32_t gr[256];
     for (uint32_t j = threadIdx.x; j < glen; j += blockDim.x) gr[j] = d_rs ? lagrange_at(d_rs, nch, j) : args.gr[j];
@@ -762,7 +785,7 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
         for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
     for (uint32_t i = 0; i + 1 < n && i < 32; ++i) args.sks[i] = sks[i];
     const unsigned threads = std::min<unsigned>(256, ((nq + 31) / 32) * 32);
-    LGK_LAUNCH(L, "induce_setup", k_induce_setup<<<1, threads, 0, L.stream>>>(d_rows, glen, d_q, nq, alpha, n, args,
+    LGK_LAUNCH(L, "induce_setup", launch_k(k_induce_setup, 1, threads, 0, L.stream, d_rows, glen, d_q, nq, alpha, n, args,
                                                                            d_S, d_apow, d_sum, d_rs,
                                                                            ilog2u(glen), d_alpha));
     return cudaGetLastError();
@@ -770,6 +793,7 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
 
 __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__restrict__ apow, uint32_t n,
                               uint32_t b, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi) {
+    pdl_begin();
     const uint32_t k = blockIdx.x;
     const uint32_t *Sk = S + (uint64_t)k * n;
     const uint32_t nlo = 1u << b, nhi = 1u << (n - b);
@@ -791,6 +815,7 @@ template <int ACC>  // ACC = max(1, 2^b / 32) words per lane
 __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
                                                      uint32_t n, uint32_t b, uint32_t nq, uint32_t qs,
                                                      uint32_t *__restrict__ out, int atomic_out) {
+    pdl_begin();
     __shared__ __align__(128) uint32_t tabs[8][kTabWords];
     __shared__ uint32_t red[32 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -827,14 +852,14 @@ __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict_
 
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
                          uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out) {
-    LGK_LAUNCH(L, "induce_prep", k_induce_prep<<<nq, 256, 0, L.stream>>>(d_S, d_apow, n, p.b, d_lo, d_hi));
+    LGK_LAUNCH(L, "induce_prep", launch_k(k_induce_prep, nq, 256, 0, L.stream, d_S, d_apow, n, p.b, d_lo, d_hi));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 grid(1u << (n - p.b), p.qsplit);
     const int ao = p.qsplit > 1;
     switch (std::max<uint32_t>(1, (1u << p.b) / 32)) {
 #define LGK_CASE(a) \
-    case a: LGK_LAUNCH(L, "induce_main", k_induce_main<a><<<grid, 256, 0, L.stream>>>(d_lo, d_hi, n, p.b, nq, p.qsplit, out, ao)); break;
+    case a: LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main<a>, grid, 256, 0, L.stream, d_lo, d_hi, n, p.b, nq, p.qsplit, out, ao)); break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(4) LGK_CASE(8) LGK_CASE(16) LGK_CASE(32)
 #undef LGK_CASE
         default: return cudaErrorInvalidValue;
@@ -844,6 +869,7 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
 
 // ============================================================== splitmix
 __global__ void k_splitmix(uint64_t seed, uint32_t *out, uint64_t n) {
+    pdl_begin();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
         z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -853,7 +879,7 @@ __global__ void k_splitmix(uint64_t seed, uint32_t *out, uint64_t n) {
 }
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n) {
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 16));
-    LGK_LAUNCH(L, "splitmix", k_splitmix<<<blocks, 256, 0, L.stream>>>(seed, out, n));
+    LGK_LAUNCH(L, "splitmix", launch_k(k_splitmix, blocks, 256, 0, L.stream, seed, out, n));
     return cudaGetLastError();
 }
 

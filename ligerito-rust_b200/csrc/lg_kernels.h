@@ -42,6 +42,28 @@ struct Launcher {
     void release();
 };
 
+// Kernel launch with programmatic dependent launch: the kernel may begin
+// launching while the previous kernel on the stream finishes; every kernel
+// of this library starts with pdl_begin() (lg_device.cuh), which waits for
+// the previous grid's completion before touching memory.  LG_PDL=0 in the
+// environment turns it off.
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                     Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // A kernel launch on L's stream, counted and (when timing) bracketed.
 #define LGK_LAUNCH(L, name, ...)   \
     do {                           \
