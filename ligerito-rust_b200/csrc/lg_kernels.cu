@@ -489,47 +489,117 @@ __device__ __forceinline__ void hash_node(const uint32_t *l, const uint32_t *r, 
     for (int w = 0; w < 8; ++w) o[w] = cv[w];
 }
 
-__global__ void k_merkle_sub(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in, uint32_t c) {
+// The tree is stored leaves first, layer after layer, 8 words per node.
+// Wide layers: a thread takes 8 consecutive nodes (256 contiguous bytes)
+// and hashes the 7 nodes of the three layers above them, keeping at most
+// three pending hashes; every lane does full work, so these launches run
+// at hashing throughput.
+__device__ __forceinline__ void load_node(const uint32_t *p, uint32_t (&h)[8]) {
+    const uint4 x = reinterpret_cast<const uint4 *>(p)[0], y = reinterpret_cast<const uint4 *>(p)[1];
+    h[0] = x.x; h[1] = x.y; h[2] = x.z; h[3] = x.w; h[4] = y.x; h[5] = y.y; h[6] = y.z; h[7] = y.w;
+}
+__device__ __forceinline__ void store_node(uint32_t *p, const uint32_t (&h)[8]) {
+    reinterpret_cast<uint4 *>(p)[0] = make_uint4(h[0], h[1], h[2], h[3]);
+    reinterpret_cast<uint4 *>(p)[1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+__device__ __forceinline__ void hash_pair(const uint32_t (&l)[8], const uint32_t (&r)[8], uint32_t (&o)[8]) {
+    hash_node(l, r, o);
+}
+
+__global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in) {
     pdl_begin();
-    extern __shared__ uint32_t sm[];  // 2 * 2^c * 8 words
-    const uint32_t width = 1u << c;
-    uint32_t *cur = sm, *nxt = sm + 8 * width;
-    const uint64_t first = (uint64_t)blockIdx.x * width;
-    const uint32_t *src = tree + 8 * (in_off + first);
-    for (uint32_t w = threadIdx.x; w < 8 * width; w += blockDim.x) cur[w] = src[w];
-    __syncthreads();
-    uint64_t lay_off = in_off, lay_n = n_in;
-    for (uint32_t l = 1; l <= c; ++l) {
-        const uint32_t cnt = width >> l;
-        const uint64_t next_off = lay_off + lay_n, next_n = lay_n / 2;
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-            uint32_t h[8];
-            hash_node(cur + 16 * i, cur + 16 * i + 8, h);
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (8 * t >= n_in) return;
+    const uint64_t off1 = in_off + n_in, off2 = off1 + n_in / 2, off3 = off2 + n_in / 4;
+    const uint32_t *src = tree + 8 * (in_off + 8 * t);
+    uint32_t q[8], l[8], r[8], n01[8], n23[8];
 #pragma unroll
-            for (int w = 0; w < 8; ++w) nxt[8 * i + w] = h[w];
-            uint32_t *dst = tree + 8 * (next_off + (first >> l) + i);
-            reinterpret_cast<uint4 *>(dst)[0] = make_uint4(h[0], h[1], h[2], h[3]);
-            reinterpret_cast<uint4 *>(dst)[1] = make_uint4(h[4], h[5], h[6], h[7]);
+    for (int half = 0; half < 2; ++half) {
+        const uint32_t *s4 = src + 32 * half;  // children 4*half .. 4*half+3
+        load_node(s4, l);
+        load_node(s4 + 8, r);
+        hash_pair(l, r, n01);
+        store_node(tree + 8 * (off1 + 4 * t + 2 * half), n01);
+        load_node(s4 + 16, l);
+        load_node(s4 + 24, r);
+        hash_pair(l, r, n23);
+        store_node(tree + 8 * (off1 + 4 * t + 2 * half + 1), n23);
+        if (half == 0) {
+            hash_pair(n01, n23, q);
+            store_node(tree + 8 * (off2 + 2 * t), q);
+        } else {
+            hash_pair(n01, n23, l);
+            store_node(tree + 8 * (off2 + 2 * t + 1), l);
+            hash_pair(q, l, r);
+            store_node(tree + 8 * (off3 + t), r);
         }
-        __syncthreads();
-        uint32_t *t = cur; cur = nxt; nxt = t;
-        lay_off = next_off;
-        lay_n = next_n;
+    }
+}
+
+// Narrow layers: a warp takes 2^lev consecutive nodes (lev <= 6) and climbs
+// lev layers, lane i of each layer hashing the pair its two source lanes
+// hold; one hash latency per layer.
+__global__ void __launch_bounds__(128) k_merkle_warp(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
+                                                     uint32_t lev) {
+    pdl_begin();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t per = 1ull << lev;
+    if (w * per >= n_in) return;  // whole warps only: n_in is a multiple of per
+    uint32_t h[8];
+    uint64_t off = in_off, n = n_in, first = w * per;  // first node of this warp in the layer
+    // first layer up: lane i < per/2 hashes nodes 2i, 2i+1 of the warp's run
+    {
+        uint32_t l[8], r[8];
+        const bool act = lane < per / 2;
+        if (act) {
+            load_node(tree + 8 * (off + first + 2 * lane), l);
+            load_node(tree + 8 * (off + first + 2 * lane + 1), r);
+            hash_pair(l, r, h);
+            store_node(tree + 8 * (off + n + first / 2 + lane), h);
+        }
+        off += n;
+        n >>= 1;
+        first >>= 1;
+    }
+    for (uint32_t k = 1; k < lev; ++k) {
+        const uint32_t cnt = (uint32_t)(per >> (k + 1));  // nodes made at this layer
+        uint32_t l[8], r[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            l[j] = __shfl_sync(0xffffffffu, h[j], (2 * lane) & 31);
+            r[j] = __shfl_sync(0xffffffffu, h[j], (2 * lane + 1) & 31);
+        }
+        if (lane < cnt) {
+            hash_pair(l, r, h);
+            store_node(tree + 8 * (off + n + first / 2 + lane), h);
+        }
+        off += n;
+        n >>= 1;
+        first >>= 1;
     }
 }
 
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
+    if (num_leaves == 0 || (num_leaves & (num_leaves - 1))) return cudaErrorInvalidValue;
     uint64_t off = 0, n = num_leaves;
     while (n > 1) {
-        const uint32_t c = std::min<uint32_t>(ilog2u(n), 8);
-        const uint32_t width = 1u << c;
-        const unsigned blocks = (unsigned)(n / width);
-        const unsigned threads = std::max<unsigned>(32, std::min<unsigned>(width / 2, 128));
-        const size_t smem = 2ull * width * 8 * sizeof(uint32_t);
-        LGK_LAUNCH(L, "merkle_layers", launch_k(k_merkle_sub, blocks, threads, smem, L.stream, tree, off, n, c));
-        cudaError_t e = cudaGetLastError();
+        cudaError_t e;
+        if (n >= (1ull << 18)) {
+            const uint64_t threads = n / 8;
+            LGK_LAUNCH(L, "merkle_thread3", launch_k(k_merkle_thread3, (unsigned)((threads + 127) / 128), 128, 0,
+                                                     L.stream, tree, off, n));
+            e = cudaGetLastError();
+            for (int l = 0; l < 3; ++l) { off += n; n /= 2; }
+        } else {
+            const uint32_t lev = std::min<uint32_t>(6, ilog2u(n));
+            const uint64_t warps = n >> lev;
+            LGK_LAUNCH(L, "merkle_warp", launch_k(k_merkle_warp, (unsigned)((warps * 32 + 127) / 128), 128, 0,
+                                                  L.stream, tree, off, n, lev));
+            e = cudaGetLastError();
+            for (uint32_t l = 0; l < lev; ++l) { off += n; n /= 2; }
+        }
         if (e != cudaSuccess) return e;
-        for (uint32_t l = 0; l < c; ++l) { off += n; n /= 2; }
     }
     return cudaSuccess;
 }
