@@ -791,7 +791,7 @@ InducePlan induce_plan(uint32_t n, uint32_t nq) {
     p.b = std::min<uint32_t>(n, 10);
     const uint64_t blocks_t = 1ull << (n - p.b);
     uint32_t qs = 1;
-    while (blocks_t * qs < 296 && qs * 16 < nq) qs *= 2;
+    while (blocks_t * qs < 3 * 296 && qs * 16 < nq) qs *= 2;  // about 3 waves of 2 blocks per SM
     p.qsplit = qs;
     p.needs_zero = qs > 1;
     return p;
@@ -891,19 +891,36 @@ __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict_
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t tb = blockIdx.x, nlo = 1u << b, nhi = 1u << (n - b);
     const uint32_t per = (nq + qs - 1) / qs, k0 = blockIdx.y * per, k1 = min(nq, k0 + per);
-    uint32_t acc[ACC];
+    uint32_t acc[ACC], cur[ACC], nxt[ACC];
 #pragma unroll
-    for (int c = 0; c < ACC; ++c) acc[c] = 0;
-    for (uint32_t k = k0 + warp; k < k1; k += nw) {
-        tab_build_warp(tabs[warp], __ldg(hi + (uint64_t)k * nhi + tb), lane);
-        __syncwarp();
+    for (int c = 0; c < ACC; ++c) acc[c] = cur[c] = nxt[c] = 0;
+    // the next query's Hi value and Lo vector are loaded while the current
+    // one is multiplied (the loads come from L2 and would otherwise stall)
+    auto load = [&](uint32_t k, uint32_t (&v)[ACC]) {
         const uint32_t *lk = lo + (uint64_t)k * nlo;
 #pragma unroll
         for (int c = 0; c < ACC; ++c) {
             const uint32_t u = lane + 32 * c;
-            if (u < nlo) acc[c] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * warp, 0, __ldg(lk + u));
+            if (u < nlo) v[c] = __ldg(lk + u);
+        }
+        return __ldg(hi + (uint64_t)k * nhi + tb);
+    };
+    uint32_t k = k0 + warp, hcur = 0;
+    if (k < k1) hcur = load(k, cur);
+    for (; k < k1; k += nw) {
+        uint32_t hnxt = 0;
+        if (k + nw < k1) hnxt = load(k + nw, nxt);
+        tab_build_warp(tabs[warp], hcur, lane);
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < ACC; ++c) {
+            const uint32_t u = lane + 32 * c;
+            if (u < nlo) acc[c] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * warp, 0, cur[c]);
         }
         __syncwarp();
+        hcur = hnxt;
+#pragma unroll
+        for (int c = 0; c < ACC; ++c) cur[c] = nxt[c];
     }
     for (uint32_t w = threadIdx.x; w < nlo; w += blockDim.x) red[w] = 0;
     __syncthreads();
