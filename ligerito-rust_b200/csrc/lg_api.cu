@@ -401,13 +401,13 @@ void induce_dev(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *d_rows, uint
     std::vector<uint32_t> sks = lg::eval_sk_at_vks(1ull << n);
     lgk::InducePlan plan = lgk::induce_plan(n, nq);
     uint32_t *d_S = static_cast<uint32_t *>(sc.dev(4ull * nq * std::max<uint32_t>(n, 1)));
-    uint32_t *d_apow = static_cast<uint32_t *>(sc.dev(4ull * nq));
+    uint32_t *d_apow = static_cast<uint32_t *>(sc.dev(8ull * nq));
     uint32_t *d_lo = static_cast<uint32_t *>(sc.dev(4ull * nq << plan.b));
     uint32_t *d_hi = static_cast<uint32_t *>(sc.dev(4ull * nq << (n - plan.b)));
     CK(c, lgk::induce_setup(c->L, d_rows, 1u << nch, d_vch ? nullptr : gr.data(), d_q, nq, alpha, n, sks.data(), d_S,
-                            d_apow, d_sum, d_vch, d_alpha));
+                            d_apow, d_vch, d_alpha));
     if (plan.needs_zero) CK(c, cudaMemsetAsync(d_out, 0, 4ull << n, c->stream));
-    CK(c, lgk::induce_basis(c->L, plan, d_S, d_apow, n, nq, d_lo, d_hi, d_out));
+    CK(c, lgk::induce_basis(c->L, plan, d_S, d_apow, n, nq, d_lo, d_hi, d_out, d_sum));
 }
 
 // host rows / queries (verifier, kernel-level API) -> induce_dev

@@ -797,36 +797,43 @@ InducePlan induce_plan(uint32_t n, uint32_t nq) {
     return p;
 }
 
-// Per-query setup of induce_sumcheck_poly_parallel, one block:
-//   dot_k = <row_k, gr> (rows gathered on the device), apow_k = alpha^k
-//   (precompute_alpha_powers, src/sumcheck_polys.rs:6-20),
+// Per-query setup of induce_sumcheck_poly_parallel, one warp per query:
+//   dot_k = <row_k, gr> (rows gathered on the device; lanes split the row),
+//   apow_k = alpha^k (precompute_alpha_powers, src/sumcheck_polys.rs:6-20;
+//   lane i holds alpha^(2^i) and the set bits of k are multiplied together),
 //   S_k[0] = q_k, S_k[i] = next_s(S_k[i-1], sks[i-1]) (sks_at_x,
-//   src/binary_fft.rs:289-292), and enforced_sum = sum_k apow_k * dot_k.
+//   src/binary_fft.rs:289-292), and contrib_k = apow_k * dot_k, stored at
+//   apow[nq + k]; induce_prep folds the contributions into the enforced sum.
 struct InduceSetupArgs {
     uint32_t gr[256];
     uint32_t sks[32];
 };
-__global__ void k_induce_setup(const uint32_t *__restrict__ rows, uint32_t glen, const uint64_t *__restrict__ q,
-                               uint32_t nq, uint32_t alpha, uint32_t n, InduceSetupArgs args,
-                               uint32_t *__restrict__ S, uint32_t *__restrict__ apow, uint32_t *sum_out,
-                               const uint32_t *d_rs, uint32_t nch, const uint32_t *d_alpha) {
+__global__ void __launch_bounds__(128) k_induce_setup(const uint32_t *__restrict__ rows, uint32_t glen,
+                                                      const uint64_t *__restrict__ q, uint32_t nq, uint32_t alpha,
+                                                      uint32_t n, InduceSetupArgs args, uint32_t *__restrict__ S,
+                                                      uint32_t *__restrict__ apow, const uint32_t *d_rs, uint32_t nch,
+                                                      const uint32_t *d_alpha) {
     pdl_begin();
     // gr: the Lagrange basis of the challenges (from the device when given)
     __shared__ uint32_t gr[256];
     for (uint32_t j = threadIdx.x; j < glen; j += blockDim.x) gr[j] = d_rs ? lagrange_at(d_rs, nch, j) : args.gr[j];
     if (d_alpha) alpha = *d_alpha;
     __syncthreads();
-    uint32_t contrib = 0;
-    for (uint32_t k = threadIdx.x; k < nq; k += blockDim.x) {
-        uint32_t dot = 0;
-        for (uint32_t j = 0; j < glen; ++j) dot ^= gf_mul(rows[(uint64_t)k * glen + j], gr[j]);
-        uint32_t p = 1, base = alpha;
-        for (uint32_t e = k; e; e >>= 1) {
-            if (e & 1) p = gf_mul(p, base);
-            base = gf_mul(base, base);
-        }
+    const uint32_t lane = threadIdx.x & 31, k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (k >= nq) return;
+    uint32_t dot = 0;
+    for (uint32_t j = lane; j < glen; j += 32) dot ^= gf_mul(rows[(uint64_t)k * glen + j], gr[j]);
+    dot = warp_xor(dot);
+    // alpha^k for k < 2^16
+    uint32_t a2 = alpha;
+    for (uint32_t i = 0; i < lane && i < 16; ++i) a2 = gf_mul(a2, a2);
+    uint32_t p = (lane < 16 && ((k >> lane) & 1)) ? a2 : 1u;
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) p = gf_mul(p, __shfl_xor_sync(0xffffffffu, p, o));
+    p = __shfl_sync(0xffffffffu, p, 0);
+    if (lane == 0) {
         apow[k] = p;
-        contrib ^= gf_mul(dot, p);
+        apow[nq + k] = gf_mul(dot, p);
         if (n) {
             uint32_t sx = (uint32_t)q[k];
             S[(uint64_t)k * n] = sx;
@@ -836,48 +843,53 @@ __global__ void k_induce_setup(const uint32_t *__restrict__ rows, uint32_t glen,
             }
         }
     }
-    __shared__ uint32_t red;
-    if (threadIdx.x == 0) red = 0;
-    __syncthreads();
-    contrib = warp_xor(contrib);
-    if ((threadIdx.x & 31) == 0) atomicXor(&red, contrib);
-    __syncthreads();
-    if (threadIdx.x == 0) *sum_out = red;
 }
 
 cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
                          const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
-                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum, const uint32_t *d_rs,
-                         const uint32_t *d_alpha) {
-    if (glen > 256 || n > 32 || nq == 0 || (glen & (glen - 1)) || (!gr && !d_rs)) return cudaErrorInvalidValue;
+                         uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs, const uint32_t *d_alpha) {
+    if (glen > 256 || n > 32 || nq == 0 || nq > 65536 || (glen & (glen - 1)) || (!gr && !d_rs))
+        return cudaErrorInvalidValue;
     InduceSetupArgs args{};
     if (!d_rs)
         for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
     for (uint32_t i = 0; i + 1 < n && i < 32; ++i) args.sks[i] = sks[i];
-    const unsigned threads = std::min<unsigned>(256, ((nq + 31) / 32) * 32);
-    LGK_LAUNCH(L, "induce_setup", launch_k(k_induce_setup, 1, threads, 0, L.stream, d_rows, glen, d_q, nq, alpha, n, args,
-                                                                           d_S, d_apow, d_sum, d_rs,
-                                                                           ilog2u(glen), d_alpha));
+    LGK_LAUNCH(L, "induce_setup", launch_k(k_induce_setup, (nq + 3) / 4, 128, 0, L.stream, d_rows, glen, d_q, nq,
+                                           alpha, n, args, d_S, d_apow, d_rs, ilog2u(glen), d_alpha));
     return cudaGetLastError();
 }
 
+// Lo_k and Hi_k of one query per block, by doubling: entry u with top bit h
+// is entry u - 2^h times S_k[h] (Lo; Hi from apow_k and S_k[b + h]), one
+// product per entry and a block barrier per bit.  Block 0 also XORs the
+// queries' contributions into the enforced sum.
 __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__restrict__ apow, uint32_t n,
-                              uint32_t b, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi) {
+                              uint32_t b, uint32_t nq, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi,
+                              uint32_t *sum_out) {
     pdl_begin();
     const uint32_t k = blockIdx.x;
     const uint32_t *Sk = S + (uint64_t)k * n;
-    const uint32_t nlo = 1u << b, nhi = 1u << (n - b);
-    for (uint32_t u = threadIdx.x; u < nlo; u += blockDim.x) {
-        uint32_t p = 1;
-        for (uint32_t i = 0; i < b; ++i)
-            if ((u >> i) & 1) p = gf_mul(p, Sk[i]);
-        lo[(uint64_t)k * nlo + u] = p;
+    uint32_t *lk = lo + ((uint64_t)k << b), *hk = hi + ((uint64_t)k << (n - b));
+    if (threadIdx.x == 0) {
+        lk[0] = 1;
+        hk[0] = apow[k];
     }
-    for (uint32_t c = threadIdx.x; c < nhi; c += blockDim.x) {
-        uint32_t p = apow[k];
-        for (uint32_t i = 0; i < n - b; ++i)
-            if ((c >> i) & 1) p = gf_mul(p, Sk[b + i]);
-        hi[(uint64_t)k * nhi + c] = p;
+    __syncthreads();
+    for (uint32_t h = 0; h < b; ++h) {
+        const uint32_t s = Sk[h];
+        for (uint32_t u = threadIdx.x; u < (1u << h); u += blockDim.x) lk[(1u << h) + u] = gf_mul(lk[u], s);
+        __syncthreads();
+    }
+    for (uint32_t h = 0; h < n - b; ++h) {
+        const uint32_t s = Sk[b + h];
+        for (uint32_t c = threadIdx.x; c < (1u << h); c += blockDim.x) hk[(1u << h) + c] = gf_mul(hk[c], s);
+        __syncthreads();
+    }
+    if (k == 0 && threadIdx.x < 32) {
+        uint32_t x = 0;
+        for (uint32_t j = threadIdx.x; j < nq; j += 32) x ^= apow[nq + j];
+        x = warp_xor(x);
+        if (threadIdx.x == 0) *sum_out = x;
     }
 }
 
@@ -938,8 +950,9 @@ __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict_
 }
 
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
-                         uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out) {
-    LGK_LAUNCH(L, "induce_prep", launch_k(k_induce_prep, nq, 256, 0, L.stream, d_S, d_apow, n, p.b, d_lo, d_hi));
+                         uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum) {
+    LGK_LAUNCH(L, "induce_prep",
+               launch_k(k_induce_prep, nq, 256, 0, L.stream, d_S, d_apow, n, p.b, nq, d_lo, d_hi, d_sum));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 grid(1u << (n - p.b), p.qsplit);

@@ -134,19 +134,22 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
 // basis[t] = sum_k apow[k] * prod_{bit i of t} S[k*n + i]; S = per-query
 // subspace values (sks_at_x).  out (2^n) must be zeroed when it returns
 // needs_zero = true.
+// The enforced sum (the sum of the setup's per-query contributions) lands
+// in d_sum (1 word).
 struct InducePlan { uint32_t b, qsplit; bool needs_zero; };
 InducePlan induce_plan(uint32_t n, uint32_t nq);
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
                          uint32_t n, uint32_t nq, uint32_t *d_scratch_lo, uint32_t *d_scratch_hi,
-                         uint32_t *out);
+                         uint32_t *out, uint32_t *d_sum);
 
 // Per-query inputs of induce_basis from device-resident opened rows
-// (nq x glen): S (nq x n), apow (nq) and the enforced sum (1 word).  gr
-// and alpha from the host, or the Lagrange basis of log2(glen) device
-// challenges d_rs and *d_alpha.
+// (nq x glen, nq <= 2^16): S (nq x n) and, in apow (2 nq words), the alpha
+// powers and each query's contribution to the enforced sum.  gr and alpha
+// from the host, or the Lagrange basis of log2(glen) device challenges
+// d_rs and *d_alpha.
 cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
                          const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
-                         uint32_t *d_S, uint32_t *d_apow, uint32_t *d_sum, const uint32_t *d_rs = nullptr,
+                         uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs = nullptr,
                          const uint32_t *d_alpha = nullptr);
 
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);

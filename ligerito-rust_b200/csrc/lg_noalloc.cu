@@ -67,7 +67,7 @@ extern "C" lg_status lg_induce_sumcheck_poly_noalloc(void *stream, uint32_t n, c
         return LG_ERR_INVALID_ARGUMENT;
     const lgk::InducePlan plan = lgk::induce_plan(n, nrows);
     const uint64_t w_S = round256((uint64_t)nrows * (n ? n : 1));
-    const uint64_t w_apow = round256(nrows);
+    const uint64_t w_apow = round256(2ull * nrows);
     const uint64_t w_lo = round256((uint64_t)nrows << plan.b);
     const uint64_t w_hi = round256((uint64_t)nrows << (n - plan.b));
     if (nrows > 256 || n > 20 || w_S + w_apow + w_lo + w_hi > kScratchWords) return LG_ERR_EXCEEDS_STATIC_SCRATCH;
@@ -101,11 +101,12 @@ extern "C" lg_status lg_induce_sumcheck_poly_noalloc(void *stream, uint32_t n, c
 
     lgk::Launcher L;
     L.stream = static_cast<cudaStream_t>(stream);
-    err = lgk::induce_setup(L, d_rows, 1u << nch, gr, d_queries, nrows, alpha, n, sks, d_S, d_apow, d_enforced_sum);
+    err = lgk::induce_setup(L, d_rows, 1u << nch, gr, d_queries, nrows, alpha, n, sks, d_S, d_apow);
     // The output is accumulated across query groups when the plan splits
     // them, so it must start at zero; the scratch regions are fully written
     // before they are read and need no clearing.
     if (err == cudaSuccess && plan.needs_zero) err = cudaMemsetAsync(d_basis_out, 0, 4ull << n, L.stream);
-    if (err == cudaSuccess) err = lgk::induce_basis(L, plan, d_S, d_apow, n, nrows, d_lo, d_hi, d_basis_out);
+    if (err == cudaSuccess)
+        err = lgk::induce_basis(L, plan, d_S, d_apow, n, nrows, d_lo, d_hi, d_basis_out, d_enforced_sum);
     return err == cudaSuccess ? LG_OK : LG_ERR_CUDA;
 }
