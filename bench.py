@@ -242,6 +242,17 @@ def run_ours(args):
                 "gf_mults_per_launch": mults,
                 "gf_mults_per_s": round(mults / avg_s, 1) if mults else None,
                 "kernel_ms": {k: round(v[1], 4) for k, v in sorted(stats.items(), key=lambda kv: -kv[1][1])}}
+    if mults:
+        # The FFT passes are not HBM-bound: every multiply is 8 table
+        # lookups in shared memory, and a conflict-free warp lookup is one
+        # 128-byte wavefront, of which an SM serves one per clock.
+        sm_hz = float((clocks or {}).get("sm_mhz") or 1965.0) * 1e6
+        wf = mults / 32 * 8 / avg_s / 1e9
+        wf_peak = 148 * sm_hz / 1e9
+        roofline["secondary"] = {"bound": "shared-memory table lookups", "achieved": round(wf, 1),
+                                 "peak": round(wf_peak, 1), "unit": "G wavefronts/s",
+                                 "frac": round(wf / wf_peak, 4),
+                                 "peak_basis": "148 SMs x 1 wavefront/clock at the sampled SM clock"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
