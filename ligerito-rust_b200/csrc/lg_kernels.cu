@@ -229,13 +229,14 @@ __global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
 // into shared memory with an odd column stride (2^K + 1 words), so both a
 // lane-per-vector walk down a column and a lane-per-row walk across the
 // columns are bank-conflict free.  All warps build the 2^K - 1 tables, then
-// the stages run in two register phases: KA = K-4 stages on 2^KA-value
-// pencils (rows u + 16i), then 4 stages on 16 contiguous rows.  Lanes run
-// over vectors, so a warp shares every table it reads.
+// the stages run in two register phases of about K/2 stages each.  Lanes
+// run over vectors, so a warp shares every table it reads; the block has
+// as many threads as a phase has pencils (up to 256), so a tile of few
+// vectors still keeps every thread busy.
 template <int K, bool INV>
 __global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
     pdl_begin();
-    constexpr int KA = K - 4, R = 1 << K, STRIDE = R + 1, CPC = R / 4;
+    constexpr int KA = K / 2, KB = K - KA, RB = 1 << KB, R = 1 << K, STRIDE = R + 1, CPC = R / 4;
     extern __shared__ __align__(16) uint8_t smraw[];
     const unsigned chunk = blockIdx.x % a.nchunks, rest = blockIdx.x / a.nchunks;
     const unsigned P = rest & ((1u << a.d0) - 1);
@@ -254,33 +255,33 @@ __global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
     }
     __syncthreads();
 
-    // work items over (vector, piece) with the vector index in the low bits
-    // (a power-of-two span, so the split is a mask and a shift)
+    // Two register phases: KA stages on pencils of 2^KA values at stride
+    // 2^KB, then KB stages on contiguous pencils of 2^KB values.  Work items
+    // run over (vector, pencil) with the vector index in the low bits (a
+    // power-of-two span, so the split is a mask and a shift).
     const uint32_t lnv = 32 - __clz(nvec - 1), vmask = (1u << lnv) - 1;
     auto phase_a = [&]() {
-        if constexpr (KA > 0) {
-            for (uint32_t item = threadIdx.x; item < (16u << lnv); item += blockDim.x) {
-                const uint32_t j = item & vmask, u = item >> lnv;
-                if (j >= nvec) continue;
-                uint32_t v[1 << KA];
+        for (uint32_t item = threadIdx.x; item < ((uint32_t)RB << lnv); item += blockDim.x) {
+            const uint32_t j = item & vmask, u = item >> lnv;
+            if (j >= nvec) continue;
+            uint32_t v[1 << KA];
 #pragma unroll
-                for (int i = 0; i < (1 << KA); ++i) v[i] = tile[j * STRIDE + u + 16 * i];
-                pencil_stages<KA, 0, INV>(v, smraw, tb, 0);
+            for (int i = 0; i < (1 << KA); ++i) v[i] = tile[j * STRIDE + u + RB * i];
+            pencil_stages<KA, 0, INV>(v, smraw, tb, 0);
 #pragma unroll
-                for (int i = 0; i < (1 << KA); ++i) tile[j * STRIDE + u + 16 * i] = v[i];
-            }
+            for (int i = 0; i < (1 << KA); ++i) tile[j * STRIDE + u + RB * i] = v[i];
         }
     };
     auto phase_b = [&]() {
         for (uint32_t item = threadIdx.x; item < ((1u << KA) << lnv); item += blockDim.x) {
             const uint32_t j = item & vmask, gq = item >> lnv;
             if (j >= nvec) continue;
-            uint32_t v[16];
+            uint32_t v[RB];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = tile[j * STRIDE + 16 * gq + i];
-            pencil_stages<4, KA, INV>(v, smraw, tb, gq);
+            for (int i = 0; i < RB; ++i) v[i] = tile[j * STRIDE + RB * gq + i];
+            pencil_stages<KB, KA, INV>(v, smraw, tb, gq);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) tile[j * STRIDE + 16 * gq + i] = v[i];
+            for (int i = 0; i < RB; ++i) tile[j * STRIDE + RB * gq + i] = v[i];
         }
     };
     if (!INV) {
@@ -328,11 +329,15 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
     char nmbuf[48];
     std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_tail" : "fft_tail", a.L, K, a.nvec);
     const size_t smem = tail_smem(K, a.vchunk);
+    uint32_t vp2 = 1;
+    while (vp2 < a.vchunk) vp2 <<= 1;
+    // pencils per phase: vectors x 2^(K - K/2) (the larger phase)
+    const unsigned threads = std::max<unsigned>(32, std::min<unsigned>(256, vp2 << (K - K / 2)));
     switch (K) {
 #define LGK_CASE(k)                                                                                 \
     case k:                                                                                         \
         cudaFuncSetAttribute(k_fft_tail<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_tail<k, INV>, blocks, 256, smem, L.stream, a));               \
+        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_tail<k, INV>, blocks, threads, smem, L.stream, a));           \
         break;
         LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
