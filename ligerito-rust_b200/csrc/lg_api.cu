@@ -253,12 +253,15 @@ Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
 
 // The first commitment of a proof whose polynomial is on the host: the
 // columns travel in groups of 16 on the copy stream; the compute stream
-// waits for each group and, while the next group is in flight, encodes it
-// (scale-and-spread and FFT treat columns independently) and runs its
-// BLAKE3 block of every leaf: a leaf is the row's words in column order and
-// 16 words are one BLAKE3 block, so group g is block g of each leaf's
-// chunk, chained through the leaf slots of the tree.  After the last group
-// only the upper tree remains.
+// waits for each group and, while the next group is in flight, runs its
+// scale-and-spread and the FFT passes but the last (columns are
+// independent).  Each pair of groups then gets the last FFT pass and its
+// BLAKE3 blocks of every leaf: a leaf is the row's words in column order
+// and 16 words are one BLAKE3 block, so group g is block g of each leaf's
+// chunk, chained through the leaf slots of the tree.  Pairs, because the
+// last pass builds its node tables per tile of vectors and 32 columns
+// share them better than 16.  After the last pair only the upper tree
+// remains.
 Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_t *d_poly, uint32_t log_m,
                          uint32_t n) {
     const Code &code = get_code(c, log_m);
@@ -305,8 +308,13 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
         CK(c, cudaStreamWaitEvent(c->stream, c->copy_ev[g % 4], 0));
         uint32_t *Eg = w.E.u32() + (uint64_t)j0 * rows;
         CK(c, lgk::rs_scale_spread(c->L, d_poly + (uint64_t)j0 * m, code.pis, Eg, log_m, cols));
-        CK(c, lgk::fft_vectors(c->L, Eg, code.tw, log_m, cols, rows, 4, m, 4, false));
-        CK(c, lgk::leaf_hash_block(c->L, w.E.u32(), rows, n, g, w.tree.u32()));
+        CK(c, lgk::fft_vectors(c->L, Eg, code.tw, log_m, cols, rows, 4, m, 4, false, lgk::FFT_HEAD));
+        if (g % 2 == 1 || g + 1 == ngroups) {
+            const uint32_t gp = g - g % 2, jp = gp * group, pcols = j0 + cols - jp;
+            CK(c, lgk::fft_vectors(c->L, w.E.u32() + (uint64_t)jp * rows, code.tw, log_m, pcols, rows, 4, m, 4, false,
+                                   lgk::FFT_LAST));
+            CK(c, lgk::leaf_hash_block(c->L, w.E.u32(), rows, n, gp, g - gp + 1, w.tree.u32()));
+        }
     }
     CK(c, lgk::merkle_upper(c->L, w.tree.u32(), rows));
     return w;

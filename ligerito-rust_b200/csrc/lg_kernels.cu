@@ -348,8 +348,9 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
 
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse) {
+                        uint32_t root_base, bool inverse, FftPasses passes) {
     if (log_len == 0 || nvec == 0) return cudaSuccess;
+    if (inverse && passes != FFT_ALL) return cudaErrorInvalidValue;
     // the roots root_base + q (q < Q) must share one heap layer
     const uint32_t lr = 31 - __builtin_clz(root_base);
     if (!L.dtab || root_base == 0 || ((root_base + Q - 1) >> lr) != 1) return cudaErrorInvalidValue;
@@ -376,6 +377,7 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
     const bool aligned = ((uintptr_t)data % 16 == 0) && (col_stride % 4 == 0) && (q_stride % 4 == 0);
     for (uint32_t pi = 0; pi < np; ++pi) {
         const uint32_t p = inverse ? np - 1 - pi : pi;
+        if ((passes == FFT_HEAD && p == np - 1) || (passes == FFT_LAST && p != np - 1)) continue;
         const uint32_t K = ks[p], d0 = d0s[p];
         PassArgs a;
         a.data = data; a.tw = tw; a.col_stride = col_stride; a.q_stride = q_stride;
@@ -437,40 +439,42 @@ __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint3
     o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
 }
 
-__global__ void k_leaf_block(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols, uint32_t b,
-                             uint32_t *__restrict__ out) {
+__global__ void k_leaf_block(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols, uint32_t b0,
+                             uint32_t nb_run, uint32_t *__restrict__ out) {
     pdl_begin();
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const uint32_t nb = (ncols + 15) / 16;
     uint4 *o = reinterpret_cast<uint4 *>(out + 8 * i);
     uint32_t cv[8];
-    if (b == 0) {
+    if (b0 == 0) {
         b3_iv(cv);
     } else {
         const uint4 x = o[0], y = o[1];
         cv[0] = x.x; cv[1] = x.y; cv[2] = x.z; cv[3] = x.w;
         cv[4] = y.x; cv[5] = y.y; cv[6] = y.z; cv[7] = y.w;
     }
-    uint32_t m[16];
+    for (uint32_t b = b0; b < b0 + nb_run; ++b) {
+        uint32_t m[16];
 #pragma unroll
-    for (int w = 0; w < 16; ++w) {
-        const uint32_t j = b * 16 + w;
-        m[w] = j < ncols ? __ldg(E + (uint64_t)j * rows + i) : 0u;
+        for (int w = 0; w < 16; ++w) {
+            const uint32_t j = b * 16 + w;
+            m[w] = j < ncols ? __ldg(E + (uint64_t)j * rows + i) : 0u;
+        }
+        const bool last = b + 1 == nb;
+        const uint32_t blen = last ? 4 * ncols - 64 * (nb - 1) : 64;
+        const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
+        b3_compress(cv, m, blen, flags);
     }
-    const bool last = b + 1 == nb;
-    const uint32_t blen = last ? 4 * ncols - 64 * (nb - 1) : 64;
-    const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
-    b3_compress(cv, m, blen, flags);
     o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
     o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
 }
 
-cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t b,
-                            uint32_t *out) {
-    if (ncols == 0 || ncols > 256 || b >= (ncols + 15) / 16) return cudaErrorInvalidValue;
+cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t b0,
+                            uint32_t nb, uint32_t *out) {
+    if (ncols == 0 || ncols > 256 || nb == 0 || b0 + nb > (ncols + 15) / 16) return cudaErrorInvalidValue;
     const unsigned blocks = (unsigned)((rows + 127) / 128);
-    LGK_LAUNCH(L, "leaf_hash_block", launch_k(k_leaf_block, blocks, 128, 0, L.stream, E, rows, ncols, b, out));
+    LGK_LAUNCH(L, "leaf_hash_block", launch_k(k_leaf_block, blocks, 128, 0, L.stream, E, rows, ncols, b0, nb, out));
     return cudaGetLastError();
 }
 

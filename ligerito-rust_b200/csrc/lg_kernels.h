@@ -86,18 +86,24 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
 // `tw` (heap order, tw[idx-1]).
 // The twiddle arrays must stay allocated and unchanged for the Launcher's
 // lifetime (its cached pass tables are keyed by their address).
+// passes: FFT_ALL, FFT_HEAD (every pass but the last), FFT_LAST (only the
+// last; forward only) -- vectors are independent, so a caller may run the
+// head passes on column groups as they arrive and the last pass on larger
+// batches.
+enum FftPasses { FFT_ALL = 0, FFT_HEAD = 1, FFT_LAST = 2 };
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse);
+                        uint32_t root_base, bool inverse, FftPasses passes = FFT_ALL);
 
 // --- Merkle (src/merkle_tree.rs:4-60, leaves src/ligero.rs:53-68) --------
 // Leaf hash of every row of a column-major matrix (rows x ncols u32).
 cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out);
-// BLAKE3 block b (columns 16b .. 16b+15) of every leaf: chains from the
-// value in out (the IV for b = 0) and leaves the chaining value there, the
-// leaf hash after the last block.  Blocks run in order 0, 1, ...
-cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t b,
-                            uint32_t *out);
+// BLAKE3 blocks b0 .. b0+nb-1 (columns 16b .. 16b+15 each) of every leaf:
+// chains from the value in out (the IV for b0 = 0) and leaves the chaining
+// value there, the leaf hash after the last block.  Calls cover the blocks
+// in order.
+cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t b0,
+                            uint32_t nb, uint32_t *out);
 // All upper layers from the leaf layer at tree[0]; tree as 8-word nodes.
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves);
 
