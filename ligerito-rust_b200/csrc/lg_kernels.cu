@@ -354,11 +354,17 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
     // the roots root_base + q (q < Q) must share one heap layer
     const uint32_t lr = 31 - __builtin_clz(root_base);
     if (!L.dtab || root_base == 0 || ((root_base + Q - 1) >> lr) != 1) return cudaErrorInvalidValue;
-    // split log_len stages into passes of <= 6, balanced
-    const uint32_t np = (log_len + 5) / 6;
+    // Stage split: the last pass (register phases over shared-memory
+    // tiles, 32 registers, many warps per SM) takes up to 6 stages; the
+    // strided passes before it hold a 2^K-value pencil per thread, and
+    // K = 4-5 keeps twice the warps per SM of K = 6 (measured faster per
+    // stage) while still doing several stages per trip through HBM.
+    const uint32_t kt = std::min<uint32_t>(6, log_len), rem = log_len - kt;
+    const uint32_t nps = rem == 0 ? 0 : (rem <= 6 ? 1 : (rem + 4) / 5);
+    const uint32_t np = nps + 1;
     if (np > kMaxFftPasses) return cudaErrorInvalidValue;
-    std::vector<uint32_t> ks(np, log_len / np);
-    for (uint32_t i = 0; i < log_len % np; ++i) ks[i] += 1;
+    std::vector<uint32_t> ks(np, kt);
+    for (uint32_t i = 0; i < nps; ++i) ks[i] = rem / nps + (i < rem % nps ? 1 : 0);
     std::vector<uint32_t> d0s(np);
     for (uint32_t i = 0, d = 0; i < np; ++i) { d0s[i] = d; d += ks[i]; }
     // D tables of every pass; kept while the same twiddle subtree is asked

@@ -12,9 +12,9 @@ namespace lgk {
 
 // Counts every kernel launch and, when timing is on, brackets each with a
 // pair of CUDA events on the launching stream (resolved lazily).
-// An FFT of up to 2^30 points runs in at most 5 passes of <= 6 stages; a
+// An FFT of up to 2^30 points runs in at most 6 passes of <= 6 stages; a
 // pass has at most 63 node tables of 128 words.
-constexpr uint32_t kMaxFftPasses = 5;
+constexpr uint32_t kMaxFftPasses = 6;
 constexpr size_t kDtabWords = kMaxFftPasses * 63 * 128;
 
 struct Launcher {
