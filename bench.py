@@ -4,8 +4,8 @@ SplitMix64 seed 1) on B200, through liblgpu.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One step = one complete proof (commit, fold, recursive commits, sumcheck
-rounds, openings; Fiat-Shamir on the host) of a polynomial already resident
-in HBM.  Prints one JSON line (rank 0).  N > 1 (torchrun, one process per
+rounds, openings; the Fiat-Shamir transcript runs on the device until the
+final opening) of a polynomial already resident in HBM.  Prints one JSON line (rank 0).  N > 1 (torchrun, one process per
 GPU) runs independent replicas: a proof does not shard, so ranks prove
 their own polynomials and only timings are reduced (max over ranks).
 
@@ -230,11 +230,13 @@ def run_ours(args):
     name, (n_launch, tot_ms) = top
     avg_s = tot_ms / n_launch / 1e3
     # fft_pass at L=18 on the 64-column first-round matrix: every launch
-    # reads and writes the whole 4 x 2^18 x 64 word matrix once
+    # reads and writes the whole 4 x 2^18 x 64 word matrix once and does K
+    # stages of 4 x 64 x 2^17 butterflies (one GF multiply each)
     algo_bytes = 2 * 4 * (4 << 18) * 64 if name.startswith("fft_pass_L18") else None
     peak, peak_kind = _peaks()
     achieved = (algo_bytes / avg_s / 1e9) if algo_bytes else None
-    mults = (64 * 4 * (1 << 17) * 6) if name.startswith("fft_pass_L18_K6") else None  # GF mults per launch
+    k_stages = int(name.split("_K")[1].split("_")[0]) if name.startswith("fft_pass_L18_K") else None
+    mults = (64 * 4 * (1 << 17) * k_stages) if k_stages else None  # GF mults per launch
     roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1) if achieved else None,
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": round(achieved / peak, 4) if achieved else None,
