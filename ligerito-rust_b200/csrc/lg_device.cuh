@@ -115,11 +115,21 @@ __device__ __forceinline__ uint32_t rotr8(uint32_t x) { return __byte_perm(x, 0,
 __device__ __forceinline__ uint32_t rotr12(uint32_t x) { return __funnelshift_r(x, x, 12); }
 __device__ __forceinline__ uint32_t rotr7(uint32_t x) { return __funnelshift_r(x, x, 7); }
 
-#define LGD_B3G(a, b, c, d, x, y)          \
-    a = a + b + (x); d = rotr16(d ^ a);    \
-    c = c + d;       b = rotr12(b ^ c);    \
-    a = a + b + (y); d = rotr8(d ^ a);     \
-    c = c + d;       b = rotr7(b ^ c);
+// x + y*one on the multiply-add pipe: BLAKE3 is bound by the integer ALU
+// pipe (adds, XORs, rotates) while the FMA pipe idles, so with `one` a
+// runtime 1 (a kernel argument the compiler cannot fold) three of the four
+// additions of G move there.  Same sum, modulo 2^32.
+__device__ __forceinline__ uint32_t add_fma(uint32_t x, uint32_t y, uint32_t one) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(y), "r"(one), "r"(x));
+    return r;
+}
+
+#define LGD_B3G(a, b, c, d, x, y)                                   \
+    a = add_fma(add_fma(a, b, one), (x), one); d = rotr16(d ^ a);   \
+    c = add_fma(c, d, one);                    b = rotr12(b ^ c);   \
+    a = a + b + (y);                           d = rotr8(d ^ a);    \
+    c = add_fma(c, d, one);                    b = rotr7(b ^ c);
 
 // Message schedule: entry (r, i) is the message word at position i of
 // round r, i.e. the spec's permutation applied r times, as compile-time
@@ -153,7 +163,7 @@ LGD_DEF_ROW(6, 11, 15, 5, 0, 1, 9, 8, 6, 14, 10, 2, 12, 3, 4, 7, 13)
 #undef LGD_DEF_ROW
 
 template <int R>
-__device__ __forceinline__ void b3_round(uint32_t (&v)[16], const uint32_t (&m)[16]) {
+__device__ __forceinline__ void b3_round(uint32_t (&v)[16], const uint32_t (&m)[16], uint32_t one) {
     LGD_B3G(v[0], v[4], v[8], v[12], m[LGD_S(R, 0)], m[LGD_S(R, 1)])
     LGD_B3G(v[1], v[5], v[9], v[13], m[LGD_S(R, 2)], m[LGD_S(R, 3)])
     LGD_B3G(v[2], v[6], v[10], v[14], m[LGD_S(R, 4)], m[LGD_S(R, 5)])
@@ -164,18 +174,19 @@ __device__ __forceinline__ void b3_round(uint32_t (&v)[16], const uint32_t (&m)[
     LGD_B3G(v[3], v[4], v[9], v[14], m[LGD_S(R, 14)], m[LGD_S(R, 15)])
 }
 
-// cv <- first 8 words of compress(cv, m, counter = 0, blen, flags)
+// cv <- first 8 words of compress(cv, m, counter = 0, blen, flags); `one`
+// must be 1 (see add_fma).
 __device__ __forceinline__ void b3_compress(uint32_t (&cv)[8], const uint32_t (&m)[16], uint32_t blen,
-                                            uint32_t flags) {
+                                            uint32_t flags, uint32_t one) {
     uint32_t v[16] = {cv[0], cv[1], cv[2], cv[3], cv[4], cv[5], cv[6], cv[7],
                       0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au, 0u, 0u, blen, flags};
-    b3_round<0>(v, m);
-    b3_round<1>(v, m);
-    b3_round<2>(v, m);
-    b3_round<3>(v, m);
-    b3_round<4>(v, m);
-    b3_round<5>(v, m);
-    b3_round<6>(v, m);
+    b3_round<0>(v, m, one);
+    b3_round<1>(v, m, one);
+    b3_round<2>(v, m, one);
+    b3_round<3>(v, m, one);
+    b3_round<4>(v, m, one);
+    b3_round<5>(v, m, one);
+    b3_round<6>(v, m, one);
 #pragma unroll
     for (int i = 0; i < 8; ++i) cv[i] = v[i] ^ v[i + 8];
 }

@@ -421,7 +421,7 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
 // Leaf = the row's n words as LE bytes, one BLAKE3 chunk (n <= 256):
 // blocks of 16 words, CHUNK_START on the first, CHUNK_END|ROOT on the last.
 __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
-                            uint32_t *__restrict__ out) {
+                            uint32_t *__restrict__ out, uint32_t one) {
     pdl_begin();
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= rows) return;
@@ -438,7 +438,7 @@ __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint3
         const bool last = b + 1 == nb;
         const uint32_t blen = last ? 4 * ncols - 64 * (nb - 1) : 64;
         const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
-        b3_compress(cv, m, blen, flags);
+        b3_compress(cv, m, blen, flags, one);
     }
     uint4 *o = reinterpret_cast<uint4 *>(out + 8 * i);
     o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
@@ -446,7 +446,7 @@ __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint3
 }
 
 __global__ void k_leaf_block(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols, uint32_t b0,
-                             uint32_t nb_run, uint32_t *__restrict__ out) {
+                             uint32_t nb_run, uint32_t *__restrict__ out, uint32_t one) {
     pdl_begin();
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= rows) return;
@@ -470,7 +470,7 @@ __global__ void k_leaf_block(const uint32_t *__restrict__ E, uint64_t rows, uint
         const bool last = b + 1 == nb;
         const uint32_t blen = last ? 4 * ncols - 64 * (nb - 1) : 64;
         const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
-        b3_compress(cv, m, blen, flags);
+        b3_compress(cv, m, blen, flags, one);
     }
     o[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
     o[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
@@ -480,26 +480,26 @@ cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint3
                             uint32_t nb, uint32_t *out) {
     if (ncols == 0 || ncols > 256 || nb == 0 || b0 + nb > (ncols + 15) / 16) return cudaErrorInvalidValue;
     const unsigned blocks = (unsigned)((rows + 127) / 128);
-    LGK_LAUNCH(L, "leaf_hash_block", launch_k(k_leaf_block, blocks, 128, 0, L.stream, E, rows, ncols, b0, nb, out));
+    LGK_LAUNCH(L, "leaf_hash_block", launch_k(k_leaf_block, blocks, 128, 0, L.stream, E, rows, ncols, b0, nb, out, 1u));
     return cudaGetLastError();
 }
 
 cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out) {
     const unsigned blocks = (unsigned)((rows + 127) / 128);
-    LGK_LAUNCH(L, "leaf_hash", launch_k(k_leaf_hash, blocks, 128, 0, L.stream, E, rows, ncols, out));
+    LGK_LAUNCH(L, "leaf_hash", launch_k(k_leaf_hash, blocks, 128, 0, L.stream, E, rows, ncols, out, 1u));
     return cudaGetLastError();
 }
 
 // Node = blake3(left || right): one 64-byte block, CHUNK_START|CHUNK_END|ROOT
 // (src/merkle_tree.rs:42-51).  A block reduces 2^c consecutive nodes of one
 // layer through c layers in shared memory and writes every layer it makes.
-__device__ __forceinline__ void hash_node(const uint32_t *l, const uint32_t *r, uint32_t *o) {
+__device__ __forceinline__ void hash_node(const uint32_t *l, const uint32_t *r, uint32_t *o, uint32_t one) {
     uint32_t m[16];
 #pragma unroll
     for (int w = 0; w < 8; ++w) { m[w] = l[w]; m[8 + w] = r[w]; }
     uint32_t cv[8];
     b3_iv(cv);
-    b3_compress(cv, m, 64, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT);
+    b3_compress(cv, m, 64, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT, one);
 #pragma unroll
     for (int w = 0; w < 8; ++w) o[w] = cv[w];
 }
@@ -517,11 +517,13 @@ __device__ __forceinline__ void store_node(uint32_t *p, const uint32_t (&h)[8]) 
     reinterpret_cast<uint4 *>(p)[0] = make_uint4(h[0], h[1], h[2], h[3]);
     reinterpret_cast<uint4 *>(p)[1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
-__device__ __forceinline__ void hash_pair(const uint32_t (&l)[8], const uint32_t (&r)[8], uint32_t (&o)[8]) {
-    hash_node(l, r, o);
+__device__ __forceinline__ void hash_pair(const uint32_t (&l)[8], const uint32_t (&r)[8], uint32_t (&o)[8],
+                                          uint32_t one) {
+    hash_node(l, r, o, one);
 }
 
-__global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in) {
+__global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
+                                                        uint32_t one) {
     pdl_begin();
     const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (8 * t >= n_in) return;
@@ -533,19 +535,19 @@ __global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ t
         const uint32_t *s4 = src + 32 * half;  // children 4*half .. 4*half+3
         load_node(s4, l);
         load_node(s4 + 8, r);
-        hash_pair(l, r, n01);
+        hash_pair(l, r, n01, one);
         store_node(tree + 8 * (off1 + 4 * t + 2 * half), n01);
         load_node(s4 + 16, l);
         load_node(s4 + 24, r);
-        hash_pair(l, r, n23);
+        hash_pair(l, r, n23, one);
         store_node(tree + 8 * (off1 + 4 * t + 2 * half + 1), n23);
         if (half == 0) {
-            hash_pair(n01, n23, q);
+            hash_pair(n01, n23, q, one);
             store_node(tree + 8 * (off2 + 2 * t), q);
         } else {
-            hash_pair(n01, n23, l);
+            hash_pair(n01, n23, l, one);
             store_node(tree + 8 * (off2 + 2 * t + 1), l);
-            hash_pair(q, l, r);
+            hash_pair(q, l, r, one);
             store_node(tree + 8 * (off3 + t), r);
         }
     }
@@ -555,7 +557,7 @@ __global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ t
 // lev layers, lane i of each layer hashing the pair its two source lanes
 // hold; one hash latency per layer.
 __global__ void __launch_bounds__(128) k_merkle_warp(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
-                                                     uint32_t lev) {
+                                                     uint32_t lev, uint32_t one) {
     pdl_begin();
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -570,7 +572,7 @@ __global__ void __launch_bounds__(128) k_merkle_warp(uint32_t *__restrict__ tree
         if (act) {
             load_node(tree + 8 * (off + first + 2 * lane), l);
             load_node(tree + 8 * (off + first + 2 * lane + 1), r);
-            hash_pair(l, r, h);
+            hash_pair(l, r, h, one);
             store_node(tree + 8 * (off + n + first / 2 + lane), h);
         }
         off += n;
@@ -586,7 +588,7 @@ __global__ void __launch_bounds__(128) k_merkle_warp(uint32_t *__restrict__ tree
             r[j] = __shfl_sync(0xffffffffu, h[j], (2 * lane + 1) & 31);
         }
         if (lane < cnt) {
-            hash_pair(l, r, h);
+            hash_pair(l, r, h, one);
             store_node(tree + 8 * (off + n + first / 2 + lane), h);
         }
         off += n;
@@ -603,14 +605,14 @@ cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
         if (n >= (1ull << 18)) {
             const uint64_t threads = n / 8;
             LGK_LAUNCH(L, "merkle_thread3", launch_k(k_merkle_thread3, (unsigned)((threads + 127) / 128), 128, 0,
-                                                     L.stream, tree, off, n));
+                                                     L.stream, tree, off, n, 1u));
             e = cudaGetLastError();
             for (int l = 0; l < 3; ++l) { off += n; n /= 2; }
         } else {
             const uint32_t lev = std::min<uint32_t>(6, ilog2u(n));
             const uint64_t warps = n >> lev;
             LGK_LAUNCH(L, "merkle_warp", launch_k(k_merkle_warp, (unsigned)((warps * 32 + 127) / 128), 128, 0,
-                                                  L.stream, tree, off, n, lev));
+                                                  L.stream, tree, off, n, lev, 1u));
             e = cudaGetLastError();
             for (uint32_t l = 0; l < lev; ++l) { off += n; n /= 2; }
         }
