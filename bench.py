@@ -270,7 +270,8 @@ def run_ours(args):
             "data": "synthetic (SplitMix64 coefficients, seed 1 + rank)",
             "config": {"workload": WORKLOAD, "log_size": 24, "parallelism": f"replicas x{world}",
                        "l2": "flushed between timed steps (write of 2 x L2)", "proof_bytes": proof_bytes},
-            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 4 * cfg.poly_len,
+            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "median_ms": round(statistics.median(e2e), 4),
+                    "min_ms": round(min(e2e), 4), "h2d_bytes_per_step": 4 * cfg.poly_len,
                     "d2h_bytes_per_step": len(pb)},
             "gpu_launches": launches,
             "clocks": clocks,
