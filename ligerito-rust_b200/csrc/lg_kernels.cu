@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
 // as many threads as a phase has pencils (up to 256), so a tile of few
 // vectors still keeps every thread busy.
 template <int K, bool INV>
-__global__ void __launch_bounds__(256) k_fft_tail(PassArgs a) {
+__global__ void __launch_bounds__(256, 4) k_fft_tail(PassArgs a) {
     pdl_begin();
     constexpr int KA = K / 2, KB = K - KA, RB = 1 << KB, R = 1 << K, STRIDE = R + 1, CPC = R / 4;
     extern __shared__ __align__(16) uint8_t smraw[];
