@@ -44,6 +44,19 @@ def test_config20_host_input_equals_device_input(lg, ctx, golden):
     assert lg.verifier(lg.hardcoded_config_20_verifier(), a, ctx)
 
 
+@pytest.mark.parametrize("k", [2, 4, 5, 7])
+def test_host_input_column_groups_match_oracle(lg, ref, ctx, k):
+    # The host-input commitment copies and encodes 16-column groups and
+    # hashes them in pairs: 4 columns (one partial group and BLAKE3 block),
+    # 16 (one group), 32 (one pair), 128 (four pairs).
+    pc = lg.ProverConfig(1, (1 << 10, 1 << k), [(1 << 6, 1 << 4)], k, [4])
+    rc = ref.config(1, 10, k, [6], [4])
+    poly = lg.splitmix_coeffs(100 + k, pc.poly_len)
+    a = lg.prover(pc, poly, ctx).to_bytes()
+    b = lg.prover(pc, lg.to_device(poly), ctx).to_bytes()
+    assert a == b == ref.prove(rc, poly, nthreads=8)
+
+
 def test_pinned_and_pageable_host_inputs_give_the_same_proof(lg, ctx):
     # the host paths overlap the input copy with the first commitment
     import torch
