@@ -219,17 +219,18 @@ def run_ours(args):
         e2e.append(a.elapsed_time(b))
     e2e_ms = rep.reduce_max(sum(e2e)) / (len(e2e) * world)
     # the floor under e2e on this box: a plain copy of the same pinned bytes
-    d_copy = torch.empty_like(poly)
+    # (torch's own stream and memory, nothing of the library involved)
+    torch.cuda.synchronize()
+    d_copy = torch.empty(cfg.poly_len, dtype=torch.int32, device=f"cuda:{dev}")
     h2d = []
     for _ in range(3):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        with torch.cuda.stream(stream):
-            d_copy.copy_(host, non_blocking=True)
-        b.record(stream)
+        a.record()
+        d_copy.copy_(host, non_blocking=True)
+        b.record()
         b.synchronize()
         h2d.append(a.elapsed_time(b))
-    del d_copy
+    torch.cuda.synchronize()
 
     # --- roofline of the dominant kernel: per-kernel CUDA events on the
     #     launching stream (a separate pass, not the timed one)

@@ -5,6 +5,7 @@
 #include "lg_kernels.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 
@@ -102,7 +103,8 @@ struct PassArgs {
     const uint4 *dtab;  // this pass's D tables (see build_pass_tables)
     uint64_t col_stride, q_stride;
     uint32_t L, d0, log_S, log_nvec_p2, nvec, log_bpg, log_B, root_base;
-    uint32_t vchunk, nchunks;  // last pass: vectors per block; both: blocks per (q, P)
+    uint32_t vchunk, nchunks;  // last pass: vectors per block, blocks per (q, P)
+    uint64_t units;            // strided passes: (group, chunk) work units
 };
 
 // The 2^K - 1 node tables of one (q, P), in 512-byte slots at the start of
@@ -190,30 +192,36 @@ __device__ __forceinline__ void pencil_stages(uint32_t (&v)[1 << KP], const uint
 // registers.  Threads of a block share (q, P) and hence every twiddle of
 // the pass; lanes run over o, so each row access is coalesced.
 template <int K, bool INV>
-__global__ void __launch_bounds__(256) k_fft_pass(PassArgs a) {
+__global__ void __launch_bounds__(256, K <= 4 ? 6 : (K == 5 ? 4 : 2)) k_fft_pass(PassArgs a) {
     pdl_begin();
     extern __shared__ __align__(16) uint8_t smraw[];
-    // block -> (q, P, first chunk); the block walks the chunks of its
-    // (q, P) with stride a.nchunks, so its tables are built once
-    const unsigned bid = blockIdx.x;
-    const unsigned c0 = bid % a.nchunks;
-    const unsigned rest = bid / a.nchunks;
-    const unsigned P = rest & ((1u << a.d0) - 1);
-    const unsigned q = rest >> a.d0;
-    build_pass_tables<K>(smraw, a, q, P);
-    const uint32_t tb = 0;
-
+    // Work units (group (q, P), chunk of 2^log_B pencils) in group-major
+    // order; block b takes the contiguous range [b U / B, (b+1) U / B), so
+    // one wave of blocks gets equal shares, and builds the node tables again
+    // only where its range enters the next group.
+    const uint32_t U = (uint32_t)a.units, nb = gridDim.x;
+    const uint32_t u0 = (uint32_t)((uint64_t)blockIdx.x * U / nb), u1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * U / nb);
     const uint64_t S = 1ull << a.log_S;
-    for (uint64_t chunk = c0; chunk < (1ull << a.log_bpg); chunk += a.nchunks) {
-        const uint64_t g = (chunk << a.log_B) + threadIdx.x;
-        const uint64_t o = g & ((1ull << a.log_S) - 1);
-        const uint64_t j = g >> a.log_S;
-        if (j >= a.nvec) break;
-        uint32_t *base = a.data + j * a.col_stride + q * a.q_stride + ((uint64_t)P << (a.L - a.d0)) + o;
+    uint32_t cur = 0xFFFFFFFFu;
+    uint32_t *gbase = a.data;
+    for (uint32_t u = u0; u < u1; ++u) {
+        const uint32_t grp = u >> a.log_bpg, chunk = u & ((1u << a.log_bpg) - 1);
+        if (grp != cur) {
+            if (cur != 0xFFFFFFFFu) __syncthreads();  // every thread is done with the old tables
+            const unsigned P = grp & ((1u << a.d0) - 1), q = grp >> a.d0;
+            build_pass_tables<K>(smraw, a, q, P);  // ends with the block synchronised
+            gbase = a.data + q * a.q_stride + ((uint64_t)P << (a.L - a.d0));
+            cur = grp;
+        }
+        const uint32_t g = (chunk << a.log_B) + threadIdx.x;
+        const uint32_t o = g & ((1u << a.log_S) - 1);
+        const uint32_t j = g >> a.log_S;
+        if (j >= a.nvec) continue;
+        uint32_t *base = gbase + j * a.col_stride + o;
         uint32_t v[1 << K];
 #pragma unroll
         for (int t = 0; t < (1 << K); ++t) v[t] = base[t * S];
-        pencil_stages<K, 0, INV>(v, smraw, tb, 0);
+        pencil_stages<K, 0, INV>(v, smraw, 0, 0);
         // recompute the store addresses instead of keeping 2^K pointers live
         uint64_t S2;
         asm volatile("mov.b64 %0, %1;" : "=l"(S2) : "l"(S));
@@ -305,18 +313,41 @@ __global__ void __launch_bounds__(256, 4) k_fft_tail(PassArgs a) {
 static size_t pass_smem(int K) { return (size_t)((1 << K) - 1) * 512; }
 static size_t tail_smem(int K, uint32_t nvec) { return pass_smem(K) + (size_t)nvec * ((1u << K) + 1) * 4; }
 
+// One wave of strided-pass blocks: as many as fit on the device at once
+// (occupancy of this instantiation, cached), at most one per unit.
+template <int K, bool INV>
+static unsigned pass_grid(uint64_t units, unsigned threads, size_t smem) {
+    static std::atomic<int> sms_c{0}, occ_c[257];  // idempotent fills; contexts may run on several threads
+    int sms = sms_c.load(std::memory_order_relaxed);
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+        sms_c.store(sms, std::memory_order_relaxed);
+    }
+    int o = occ_c[threads].load(std::memory_order_relaxed);
+    if (!o) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_fft_pass<K, INV>, (int)threads, smem) != cudaSuccess || o < 1)
+            o = 1;
+        occ_c[threads].store(o, std::memory_order_relaxed);
+    }
+    return (unsigned)std::min<uint64_t>(units, (uint64_t)sms * o);
+}
+
 template <bool INV>
-static cudaError_t launch_pass(Launcher &L, int K, PassArgs a, unsigned blocks, unsigned threads) {
+static cudaError_t launch_pass(Launcher &L, int K, PassArgs a, unsigned threads) {
     char nmbuf[48];
     std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_pass" : "fft_pass", a.L, K, a.nvec);
     const size_t smem = pass_smem(K);
     switch (K) {
 #define LGK_CASE(k)                                                                                  \
-    case k:                                                                                          \
+    case k: {                                                                                        \
         if (smem > 48 * 1024)                                                                        \
             cudaFuncSetAttribute(k_fft_pass<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_pass<k, INV>, blocks, threads, smem, L.stream, a));            \
-        break;
+        const unsigned blocks = pass_grid<k, INV>(a.units, threads, smem);                           \
+        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_pass<k, INV>, blocks, threads, smem, L.stream, a));      \
+        break;                                                                                       \
+    }
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
         default: return cudaErrorInvalidValue;
@@ -405,13 +436,9 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
         const uint32_t B = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>(G, 256));
         a.log_B = ilog2u(B);
         a.log_bpg = ilog2u(G / B);
-        // about 4 waves of resident blocks; each walks its chunks
-        const uint64_t groups = (uint64_t)Q << d0, bpg = 1ull << a.log_bpg;
-        a.nchunks = (uint32_t)std::min<uint64_t>(bpg, std::max<uint64_t>(1, (148ull * 8) / groups));
-        const uint64_t blocks = groups * a.nchunks;
-        if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidValue;
-        cudaError_t e = inverse ? launch_pass<true>(L, (int)K, a, (unsigned)blocks, B)
-                                : launch_pass<false>(L, (int)K, a, (unsigned)blocks, B);
+        a.units = ((uint64_t)Q << d0) << a.log_bpg;
+        a.nchunks = 0;
+        cudaError_t e = inverse ? launch_pass<true>(L, (int)K, a, B) : launch_pass<false>(L, (int)K, a, B);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
