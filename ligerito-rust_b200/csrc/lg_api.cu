@@ -231,12 +231,35 @@ struct Witness {  // RecursiveLigeroWitness, src/data_structures.rs:32-40
     const uint32_t *root() const { return tree.u32() + 8 * (2 * rows - 2); }  // on the device
 };
 
+// encode_non_systematic (src/reed_solomon.rs:104-113) of n columns into E
+// (column-major, 4m rows): the columns scaled by pis are written once to
+// `scaled` (n columns of m words) and the first FFT pass of all four
+// quarters reads them from there, instead of spreading four copies through
+// HBM; codes short enough for a single FFT pass spread them.
+void rs_encode(lg_ctx *c, const Code &code, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *E,
+               uint64_t col_stride, uint32_t *scaled, lgk::FftPasses passes = lgk::FFT_ALL) {
+    const uint64_t m = 1ull << log_m;
+    if (log_m > 6) {
+        CK(c, lgk::rs_scale(c->L, d_poly, code.pis, scaled, log_m, n));
+        lgk::FftSrc src;
+        src.p = scaled;
+        src.col_stride = m;
+        src.q_stride = 0;
+        CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, col_stride, 4, m, 4, false, passes, &src));
+    } else {
+        CK(c, lgk::rs_scale_spread(c->L, d_poly, code.pis, E, log_m, n));
+        CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, col_stride, 4, m, 4, false, passes));
+    }
+}
+
 // ligero_commit (src/ligero.rs:70-95) into caller buffers
 void commit_into(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *E, uint32_t *tree) {
     const Code &code = get_code(c, log_m);
     const uint64_t m = 1ull << log_m, rows = 4 * m;
-    CK(c, lgk::rs_scale_spread(c->L, d_poly, code.pis, E, log_m, n));
-    CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, rows, 4, m, 4, false));
+    {
+        DBuf scaled(c, log_m > 6 ? 4ull * n * m : 0);
+        rs_encode(c, code, d_poly, log_m, n, E, rows, scaled.u32());
+    }
     CK(c, lgk::leaf_hashes(c->L, E, rows, n, tree));
     CK(c, lgk::merkle_upper(c->L, tree, rows));
 }
@@ -275,6 +298,7 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
     const bool pinned_src = cudaPointerGetAttributes(&attr, h_poly) == cudaSuccess && attr.type == cudaMemoryTypeHost;
     cudaGetLastError();
     const uint32_t group = std::min<uint32_t>(n, 16), ngroups = (n + group - 1) / group;
+    DBuf scaled(c, log_m > 6 ? 4ull * n * m : 0);
     // staging for pageable input: two pinned chunks, reused after their copy
     constexpr size_t kChunk = 4u << 20;
     uint8_t *slot[2] = {nullptr, nullptr};
@@ -307,8 +331,8 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
         CK(c, cudaEventRecord(c->copy_ev[g % 4], c->copy_stream));
         CK(c, cudaStreamWaitEvent(c->stream, c->copy_ev[g % 4], 0));
         uint32_t *Eg = w.E.u32() + (uint64_t)j0 * rows;
-        CK(c, lgk::rs_scale_spread(c->L, d_poly + (uint64_t)j0 * m, code.pis, Eg, log_m, cols));
-        CK(c, lgk::fft_vectors(c->L, Eg, code.tw, log_m, cols, rows, 4, m, 4, false, lgk::FFT_HEAD));
+        rs_encode(c, code, d_poly + (uint64_t)j0 * m, log_m, cols, Eg, rows, scaled.u32() + (uint64_t)j0 * m,
+                  lgk::FFT_HEAD);
         if (g % 2 == 1 || g + 1 == ngroups) {
             const uint32_t gp = g - g % 2, jp = gp * group, pcols = j0 + cols - jp;
             CK(c, lgk::fft_vectors(c->L, w.E.u32() + (uint64_t)jp * rows, code.tw, log_m, pcols, rows, 4, m, 4, false,
@@ -1044,8 +1068,8 @@ lg_status lg_rs_encode_cols(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, u
     return guarded(c, [&] {
         CK(c, cudaSetDevice(c->device));
         const Code &code = get_code(c, log_m);
-        CK(c, lgk::rs_scale_spread(c->L, d_poly, code.pis, d_enc, log_m, n));
-        CK(c, lgk::fft_vectors(c->L, d_enc, code.tw, log_m, n, 4ull << log_m, 4, 1ull << log_m, 4, false));
+        DBuf scaled(c, log_m > 6 ? 4ull * n << log_m : 0);
+        rs_encode(c, code, d_poly, log_m, n, d_enc, 4ull << log_m, scaled.u32());
         sync(c);
     });
 }

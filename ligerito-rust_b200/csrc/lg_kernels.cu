@@ -84,6 +84,23 @@ __global__ void k_rs_scale_spread(const uint32_t *__restrict__ poly, const uint3
     }
 }
 
+__global__ void k_rs_scale(const uint32_t *__restrict__ poly, const uint32_t *__restrict__ pis,
+                           uint32_t *__restrict__ out, uint32_t log_m, uint64_t total) {
+    pdl_begin();
+    const uint64_t m = 1ull << log_m;
+    for (uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (uint64_t)gridDim.x * blockDim.x)
+        out[idx] = gf_mul(poly[idx], pis[idx & (m - 1)]);
+}
+
+cudaError_t rs_scale(Launcher &L, const uint32_t *poly, const uint32_t *pis, uint32_t *out, uint32_t log_m,
+                     uint32_t n) {
+    const uint64_t total = (uint64_t)n << log_m;
+    const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
+    LGK_LAUNCH(L, "rs_scale", launch_k(k_rs_scale, blocks, 256, 0, L.stream, poly, pis, out, log_m, total));
+    return cudaGetLastError();
+}
+
 cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *pis, uint32_t *E,
                             uint32_t log_m, uint32_t n) {
     uint64_t total = (uint64_t)n << log_m;
@@ -105,6 +122,8 @@ struct PassArgs {
     uint32_t L, d0, log_S, log_nvec_p2, nvec, log_bpg, log_B, root_base;
     uint32_t vchunk, nchunks;  // last pass: vectors per block, blocks per (q, P)
     uint64_t units;            // strided passes: (group, chunk) work units
+    const uint32_t *src;       // strided passes: input, when not data (FftSrc)
+    uint64_t src_col_stride, src_q_stride;
 };
 
 // The 2^K - 1 node tables of one (q, P), in 512-byte slots at the start of
@@ -204,6 +223,9 @@ __global__ void __launch_bounds__(256, K <= 4 ? 6 : (K == 5 ? 4 : 2)) k_fft_pass
     const uint64_t S = 1ull << a.log_S;
     uint32_t cur = 0xFFFFFFFFu;
     uint32_t *gbase = a.data;
+    const uint32_t *sgbase = a.data;
+    const bool own_src = a.src != nullptr;
+    const uint64_t scs = own_src ? a.src_col_stride : a.col_stride;
     for (uint32_t u = u0; u < u1; ++u) {
         const uint32_t grp = u >> a.log_bpg, chunk = u & ((1u << a.log_bpg) - 1);
         if (grp != cur) {
@@ -211,6 +233,7 @@ __global__ void __launch_bounds__(256, K <= 4 ? 6 : (K == 5 ? 4 : 2)) k_fft_pass
             const unsigned P = grp & ((1u << a.d0) - 1), q = grp >> a.d0;
             build_pass_tables<K>(smraw, a, q, P);  // ends with the block synchronised
             gbase = a.data + q * a.q_stride + ((uint64_t)P << (a.L - a.d0));
+            sgbase = own_src ? a.src + q * a.src_q_stride + ((uint64_t)P << (a.L - a.d0)) : gbase;
             cur = grp;
         }
         const uint32_t g = (chunk << a.log_B) + threadIdx.x;
@@ -218,9 +241,10 @@ __global__ void __launch_bounds__(256, K <= 4 ? 6 : (K == 5 ? 4 : 2)) k_fft_pass
         const uint32_t j = g >> a.log_S;
         if (j >= a.nvec) continue;
         uint32_t *base = gbase + j * a.col_stride + o;
+        const uint32_t *lbase = sgbase + j * scs + o;
         uint32_t v[1 << K];
 #pragma unroll
-        for (int t = 0; t < (1 << K); ++t) v[t] = base[t * S];
+        for (int t = 0; t < (1 << K); ++t) v[t] = lbase[t * S];
         pencil_stages<K, 0, INV>(v, smraw, 0, 0);
         // recompute the store addresses instead of keeping 2^K pointers live
         uint64_t S2;
@@ -379,9 +403,10 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
 
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse, FftPasses passes) {
+                        uint32_t root_base, bool inverse, FftPasses passes, const FftSrc *src) {
     if (log_len == 0 || nvec == 0) return cudaSuccess;
     if (inverse && passes != FFT_ALL) return cudaErrorInvalidValue;
+    if (src && (inverse || log_len <= 6 || passes == FFT_LAST)) return cudaErrorInvalidValue;
     // the roots root_base + q (q < Q) must share one heap layer
     const uint32_t lr = 31 - __builtin_clz(root_base);
     if (!L.dtab || root_base == 0 || ((root_base + Q - 1) >> lr) != 1) return cudaErrorInvalidValue;
@@ -419,6 +444,9 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
         PassArgs a;
         a.data = data; a.tw = tw; a.col_stride = col_stride; a.q_stride = q_stride;
         a.dtab = reinterpret_cast<const uint4 *>(L.dtab + (size_t)p * 63 * kTabWords);
+        a.src = (src && p == 0) ? src->p : nullptr;
+        a.src_col_stride = src ? src->col_stride : 0;
+        a.src_q_stride = src ? src->q_stride : 0;
         a.L = log_len; a.d0 = d0; a.log_S = log_len - d0 - K;
         a.log_nvec_p2 = ilog2u(nvec_p2); a.nvec = nvec; a.root_base = root_base;
         const bool tail = a.log_S == 0 && K >= 4 && aligned;

@@ -79,6 +79,11 @@ cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t sme
 // copies, so quarter q then needs the m-point FFT under heap node 4+q.
 cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *pis, uint32_t *E,
                             uint32_t log_m, uint32_t n);
+// The same scaling without the spread: out[j*m + i] = poly[j*m + i] * pis[i]
+// (n columns of m), for an FFT whose first pass reads all four quarters'
+// input from it (FftSrc).
+cudaError_t rs_scale(Launcher &L, const uint32_t *poly, const uint32_t *pis, uint32_t *out, uint32_t log_m,
+                     uint32_t n);
 
 // In-place additive FFT / IFFT (src/binary_fft.rs:109-206) of `nvec * Q`
 // vectors of 2^log_len: vector (j, q) starts at data + j*col_stride +
@@ -90,10 +95,18 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
 // last; forward only) -- vectors are independent, so a caller may run the
 // head passes on column groups as they arrive and the last pass on larger
 // batches.
+// src: where the first pass reads its input instead of data (vector (j, q)
+// at src + j*col_stride + q*q_stride; q_stride 0 lets all Q subtrees start
+// from one copy); the first pass must then be a strided pass (log_len > 6).
 enum FftPasses { FFT_ALL = 0, FFT_HEAD = 1, FFT_LAST = 2 };
+struct FftSrc {
+    const uint32_t *p = nullptr;
+    uint64_t col_stride = 0, q_stride = 0;
+};
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse, FftPasses passes = FFT_ALL);
+                        uint32_t root_base, bool inverse, FftPasses passes = FFT_ALL,
+                        const FftSrc *src = nullptr);
 
 // --- Merkle (src/merkle_tree.rs:4-60, leaves src/ligero.rs:53-68) --------
 // Leaf hash of every row of a column-major matrix (rows x ncols u32).

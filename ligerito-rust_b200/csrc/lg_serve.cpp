@@ -41,10 +41,11 @@ struct Request {
 };
 
 // Device bytes one proof holds at its peak: the input when it is on the
-// host, the first encoded matrix (16 bytes per coefficient) and its tree
-// (4 per coefficient), the folded vectors and the per-context arenas.
+// host, the first encoded matrix (16 bytes per coefficient), its tree (4
+// per coefficient), the scaled columns the encoding reads (4 per
+// coefficient), the folded vectors and the per-context arenas.
 uint64_t footprint(const lg_config &c, uint64_t len, int on_device) {
-    uint64_t b = 16 * len + 4 * len + (len >> c.initial_k) * 4 * 4 + (48ull << 20);
+    uint64_t b = 16 * len + 4 * len + 4 * len + (len >> c.initial_k) * 4 * 4 + (48ull << 20);
     if (!on_device) b += 4 * len;
     return b;
 }
