@@ -384,6 +384,10 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
     char nmbuf[48];
     std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_tail" : "fft_tail", a.L, K, a.nvec);
     const size_t smem = tail_smem(K, a.vchunk);
+    // the kernel's limit is always set to its largest tile: contexts on other
+    // threads launch the same kernel with other tile sizes, and a smaller
+    // limit set between another thread's set and launch would fail it
+    const int smem_max = (int)tail_smem(K, 64);
     uint32_t vp2 = 1;
     while (vp2 < a.vchunk) vp2 <<= 1;
     // pencils per phase: vectors x 2^(K - K/2) (the larger phase)
@@ -391,7 +395,7 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
     switch (K) {
 #define LGK_CASE(k)                                                                                 \
     case k:                                                                                         \
-        cudaFuncSetAttribute(k_fft_tail<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        cudaFuncSetAttribute(k_fft_tail<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);   \
         LGK_LAUNCH(L, nmbuf, launch_k(k_fft_tail<k, INV>, blocks, threads, smem, L.stream, a));           \
         break;
         LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
