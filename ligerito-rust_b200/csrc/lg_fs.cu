@@ -47,11 +47,11 @@ __global__ void k_fs_step(FsState *g, FsStep a) {
     pdl_begin();
     __shared__ FsState S;
     __shared__ Batch B;
+    __shared__ uint32_t stage[32];
     load_state(S, g);
-    if (threadIdx.x == 0) {
-        if (a.check && (a.src[0] ^ a.src[1]) != a.src[3]) S.err |= FS_ERR_SUMCHECK;
-        fs_absorb(S, a.src, a.nwords);
-    }
+    const bool bad = threadIdx.x == 0 && a.check && (a.src[0] ^ a.src[1]) != a.src[3];
+    fs_absorb_block(S, a.src, a.nwords, stage, 32);
+    if (bad) S.err |= FS_ERR_SUMCHECK;
     __syncthreads();
     fs_fields(S, B, a.nsq, a.out);
     store_state(S, g);
@@ -75,18 +75,37 @@ __device__ uint32_t block_rank(bool flag, uint32_t *scratch, uint32_t *total) {
     return before + __popc(m & ((1u << lane) - 1));
 }
 
+// At most 2 kQBlock values (the queries taken and a batch) go into a set
+// of kHash slots, so probing always ends within the table.
+constexpr uint32_t kHash = 4 * kQBlock;
+static_assert(kHash == 1024, "hash_insert takes 10 bits of the hash");
+__device__ uint32_t hash_insert(unsigned long long *key, uint32_t *rank, uint64_t v, uint32_t r) {
+    uint32_t h = ((uint32_t)(v ^ (v >> 31)) * 0x9E3779B1u) >> 22;  // 10 bits: kHash = 1024 slots
+    for (uint32_t probe = 0; probe < kHash; ++probe) {
+        const unsigned long long prev = atomicCAS(key + h, ~0ull, (unsigned long long)v);
+        if (prev == ~0ull || prev == v) {
+            atomicMin(rank + h, r);
+            return h;
+        }
+        h = (h + 1) & (kHash - 1);
+    }
+    return kHash - 1;  // unreachable: the table is never more than half full
+}
+
 __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a) {
     pdl_begin();
     __shared__ FsState S;
     __shared__ Batch B;
-    __shared__ uint64_t acc[kQBlock], cand[kQBlock];
+    __shared__ uint64_t acc[kQBlock];
+    __shared__ unsigned long long hkey[kHash];
+    __shared__ uint32_t hrank[kHash];
     __shared__ uint32_t lo32[kQBlock];
     __shared__ uint32_t scratch[kQBlock / 32];
+    __shared__ uint32_t wcnt[64][kQBlock / 32];
     __shared__ uint32_t take_sh, batch_sh;
     const uint32_t tid = threadIdx.x;
     load_state(S, g);
-    if (tid == 0) fs_absorb(S, a.src, a.nwords);
-    __syncthreads();
+    fs_absorb_block(S, a.src, a.nwords, lo32, kQBlock);
     const bool ok = a.n >= a.s && a.s >= 1 && a.s <= kQBlock;
     const uint64_t mask = a.n - 1;  // n is a power of two: % n is a mask
     uint32_t count = 0, batch = 0, take = 0;
@@ -106,11 +125,18 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a)
             lo32[tid] = (uint32_t)lo;
             qv = lo & mask;
         }
-        cand[tid] = qv;
+        // Repeats: the queries taken so far (rank 0) and this batch's
+        // squeezes (rank i + 1) go into a shared hash set that keeps each
+        // value's smallest rank; a squeeze is new iff it holds its value's.
+        for (uint32_t i = tid; i < kHash; i += blockDim.x) {
+            hkey[i] = ~0ull;  // never a value: values are < n <= 2^63
+            hrank[i] = ~0u;
+        }
         __syncthreads();
-        bool dup = tid >= batch;
-        for (uint32_t k = 0; k < count; ++k) dup |= acc[k] == qv;
-        for (uint32_t j = 0; j < tid; ++j) dup |= cand[j] == qv;
+        if (tid < count) hash_insert(hkey, hrank, acc[tid], 0);
+        const uint32_t slot = tid < batch ? hash_insert(hkey, hrank, qv, tid + 1) : 0;
+        __syncthreads();
+        const bool dup = tid >= batch || hrank[slot] != tid + 1;
         uint32_t fresh;
         const uint32_t rank = block_rank(!dup, scratch, &fresh);
         if (!dup && rank < need) acc[count + rank] = qv;
@@ -165,25 +191,68 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a)
         const uint64_t qi = have ? acc[tid] : 0;
         const uint64_t qp = have && tid > 0 ? acc[tid - 1] : ~0ull;
         const uint64_t qn = have && tid + 1 < count ? acc[tid + 1] : ~0ull;
-        uint32_t nout = 0;
-        uint64_t layer_off = 0, width = a.n;
-        for (uint32_t d = 0; (1ull << d) < a.n; ++d) {
-            bool emit = false;
-            uint64_t x = 0;
-            if (have) {
-                x = qi >> d;
-                const bool has_p = qp != ~0ull, has_n = qn != ~0ull;
-                const uint64_t xp = qp >> d, xn = qn >> d;
-                if (x & 1) emit = (!has_p || xp != x) && !(has_p && xp == (x ^ 1));
-                else emit = (!has_n || xn != x) && !(has_n && xn == (x ^ 1));
+        const uint32_t lane = tid & 31, warp = tid >> 5;
+        uint32_t nl = 0;
+        while ((1ull << nl) < a.n) ++nl;
+        auto emits = [&](uint32_t d, uint64_t &x) {
+            x = qi >> d;
+            if (!have) return false;
+            const bool has_p = qp != ~0ull, has_n = qn != ~0ull;
+            const uint64_t xp = qp >> d, xn = qn >> d;
+            if (x & 1) return (!has_p || xp != x) && !(has_p && xp == (x ^ 1));
+            return (!has_n || xn != x) && !(has_n && xn == (x ^ 1));
+        };
+        // Per-warp counts of every layer, then one scan gives each warp its
+        // start in each layer (layers in order, threads in query order):
+        // two barriers instead of two per layer.
+        uint64_t x;
+        for (uint32_t d = 0; d < nl; ++d) {
+            const uint32_t m = __ballot_sync(0xffffffffu, emits(d, x));
+            if (lane == 0) wcnt[d][warp] = __popc(m);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // lane l scans layers l and l + 32: in-layer warp offsets, then
+            // a shuffle scan of the layer totals
+            uint32_t tot[2] = {0, 0};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t d = lane + 32 * h;
+                if (d < nl)
+                    for (uint32_t w = 0; w < kQBlock / 32; ++w) {
+                        const uint32_t c = wcnt[d][w];
+                        wcnt[d][w] = tot[h];
+                        tot[h] += c;
+                    }
             }
-            uint32_t tot;
-            const uint32_t pos = nout + block_rank(emit, scratch, &tot);
-            if (emit && pos < a.nodes_cap) a.nodes[pos] = layer_off + (x ^ 1);
-            nout += tot;
+            uint32_t inc[2] = {tot[0], tot[1]};
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                for (uint32_t o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, inc[h], o);
+                    if (lane >= o) inc[h] += y;
+                }
+            const uint32_t all0 = __shfl_sync(0xffffffffu, inc[0], 31);
+            const uint32_t start[2] = {inc[0] - tot[0], all0 + inc[1] - tot[1]};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t d = lane + 32 * h;
+                if (d < nl)
+                    for (uint32_t w = 0; w < kQBlock / 32; ++w) wcnt[d][w] += start[h];
+            }
+            if (lane == 31) take_sh = all0 + inc[1];
+        }
+        __syncthreads();
+        uint64_t layer_off = 0, width = a.n;
+        for (uint32_t d = 0; d < nl; ++d) {
+            const bool e = emits(d, x);
+            const uint32_t m = __ballot_sync(0xffffffffu, e);
+            const uint32_t pos = wcnt[d][warp] + __popc(m & ((1u << lane) - 1));
+            if (e && pos < a.nodes_cap) a.nodes[pos] = layer_off + (x ^ 1);
             layer_off += width;
             width >>= 1;
         }
+        const uint32_t nout = take_sh;
         if (tid == 0) {
             *a.nnodes = nout;
             if (nout > a.nodes_cap) S.err |= FS_ERR_QUERIES;

@@ -24,21 +24,33 @@ __device__ __forceinline__ uint32_t rr(uint32_t x, int r) { return __funnelshift
 __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 
 // FIPS 180-4 compression of one block of 16 big-endian words (registers).
+// The transcript runs it on one thread or a few warps, where instruction
+// fetch rather than arithmetic sets the pace: the 64 rounds are a loop of
+// four 16-round bodies (about a third of the code of a full unroll), with
+// the next 16 schedule words computed in place after each body.
 __device__ __forceinline__ void sha_compress(uint32_t st[8], const uint32_t (&blk)[16]) {
     uint32_t w[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) w[i] = blk[i];
     uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll 1
+    for (int t0 = 0; t0 < 64; t0 += 16) {
 #pragma unroll
-    for (int t = 0; t < 64; ++t) {
-        if (t >= 16) {
-            const uint32_t x = w[(t - 15) & 15], y = w[(t - 2) & 15];
-            w[t & 15] += (rr(x, 7) ^ rr(x, 18) ^ (x >> 3)) + w[(t - 7) & 15] + (rr(y, 17) ^ rr(y, 19) ^ (y >> 10));
+        for (int i = 0; i < 16; ++i) {
+            const uint32_t hk = h + kK256[t0 + i] + w[i];  // independent of e: off the serial path
+            const uint32_t t1 = hk + (rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)) + ((e & f) ^ (~e & g));
+            const uint32_t t2 = (rr(a, 2) ^ rr(a, 13) ^ rr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+            h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
         }
-        const uint32_t hk = h + kK256[t] + w[t & 15];  // independent of e: off the serial path
-        const uint32_t t1 = hk + (rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)) + ((e & f) ^ (~e & g));
-        const uint32_t t2 = (rr(a, 2) ^ rr(a, 13) ^ rr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
-        h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+        if (t0 < 48) {
+            // W[t] = s1(W[t-2]) + W[t-7] + s0(W[t-15]) + W[t-16], in order,
+            // so words t-2 and t-7 are already the new ones where they must be
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const uint32_t x = w[(i + 1) & 15], y = w[(i + 14) & 15];
+                w[i] += (rr(x, 7) ^ rr(x, 18) ^ (x >> 3)) + w[(i + 9) & 15] + (rr(y, 17) ^ rr(y, 19) ^ (y >> 10));
+            }
+        }
     }
     st[0] += a; st[1] += b; st[2] += c; st[3] += d; st[4] += e; st[5] += f; st[6] += g; st[7] += h;
 }
@@ -56,6 +68,20 @@ __device__ void fs_absorb(FsState &S, const uint32_t *src, uint32_t nwords) {
         }
     }
     S.total += 4ull * nwords;
+}
+
+// The whole block absorbs nwords u32s from device memory: each run of up
+// to `cap` words is loaded in parallel into the shared `stage`, then
+// thread 0 absorbs it, so the words cost one memory round trip per run
+// instead of one each.
+__device__ void fs_absorb_block(FsState &S, const uint32_t *src, uint32_t nwords, uint32_t *stage, uint32_t cap) {
+    for (uint32_t base = 0; base < nwords; base += cap) {
+        const uint32_t n = min(cap, nwords - base);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) stage[i] = src[base + i];
+        __syncthreads();
+        if (threadIdx.x == 0) fs_absorb(S, stage, n);
+        __syncthreads();
+    }
 }
 
 // Word j of the pending words followed by the counters c, c+1, ... (each

@@ -209,9 +209,13 @@ __device__ __forceinline__ void pencil_stages(uint32_t (&v)[1 << KP], const uint
 // Strided passes: a thread owns one "pencil", the 2^K rows
 // P*2^(L-d0) + t*S + o (t < 2^K) of one vector, S = 2^(L-d0-K) > 1, in
 // registers.  Threads of a block share (q, P) and hence every twiddle of
-// the pass; lanes run over o, so each row access is coalesced.
+// the pass; lanes run over o, so each row access is coalesced.  With
+// K <= 4 a thread also holds the next unit's pencil, loaded before this
+// one's stages run so that its HBM latency hides behind them (64
+// registers, 4 blocks per SM: measured faster than 6 blocks without it);
+// larger pencils would spill.
 template <int K, bool INV>
-__global__ void __launch_bounds__(256, K <= 4 ? 6 : (K == 5 ? 4 : 2)) k_fft_pass(PassArgs a) {
+__global__ void __launch_bounds__(256, K <= 4 ? 4 : (K == 5 ? 4 : 2)) k_fft_pass(PassArgs a) {
     pdl_begin();
     extern __shared__ __align__(16) uint8_t smraw[];
     // Work units (group (q, P), chunk of 2^log_B pencils) in group-major
@@ -222,37 +226,71 @@ __global__ void __launch_bounds__(256, K <= 4 ? 6 : (K == 5 ? 4 : 2)) k_fft_pass
     const uint32_t u0 = (uint32_t)((uint64_t)blockIdx.x * U / nb), u1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * U / nb);
     const uint64_t S = 1ull << a.log_S;
     uint32_t cur = 0xFFFFFFFFu;
-    uint32_t *gbase = a.data;
-    const uint32_t *sgbase = a.data;
     const bool own_src = a.src != nullptr;
     const uint64_t scs = own_src ? a.src_col_stride : a.col_stride;
-    for (uint32_t u = u0; u < u1; ++u) {
+    // Pencil of unit u for this thread: load pointer, store pointer and
+    // whether the thread has a vector there (nvec need not be a power of 2).
+    auto locate = [&](uint32_t u, const uint32_t *&lb, uint32_t *&sb) -> bool {
         const uint32_t grp = u >> a.log_bpg, chunk = u & ((1u << a.log_bpg) - 1);
+        const unsigned P = grp & ((1u << a.d0) - 1), q = grp >> a.d0;
+        const uint64_t row0 = (uint64_t)P << (a.L - a.d0);
+        const uint32_t g = (chunk << a.log_B) + threadIdx.x;
+        const uint32_t o = g & ((1u << a.log_S) - 1), j = g >> a.log_S;
+        sb = a.data + q * a.q_stride + row0 + j * a.col_stride + o;
+        lb = own_src ? a.src + q * a.src_q_stride + row0 + j * scs + o : sb;
+        return j < a.nvec;
+    };
+    constexpr bool PF = K <= 4;
+    constexpr int NP = PF ? (1 << K) : 1;
+    uint32_t v[1 << K], nv[NP];
+    const uint32_t *lb;
+    uint32_t *sb;
+    bool have = PF && u0 < u1 && locate(u0, lb, sb);
+    if (PF && have) {
+#pragma unroll
+        for (int t = 0; t < NP; ++t) nv[t] = lb[t * S];
+    }
+    for (uint32_t u = u0; u < u1; ++u) {
+        const uint32_t grp = u >> a.log_bpg;
         if (grp != cur) {
             if (cur != 0xFFFFFFFFu) __syncthreads();  // every thread is done with the old tables
             const unsigned P = grp & ((1u << a.d0) - 1), q = grp >> a.d0;
             build_pass_tables<K>(smraw, a, q, P);  // ends with the block synchronised
-            gbase = a.data + q * a.q_stride + ((uint64_t)P << (a.L - a.d0));
-            sgbase = own_src ? a.src + q * a.src_q_stride + ((uint64_t)P << (a.L - a.d0)) : gbase;
             cur = grp;
         }
-        const uint32_t g = (chunk << a.log_B) + threadIdx.x;
-        const uint32_t o = g & ((1u << a.log_S) - 1);
-        const uint32_t j = g >> a.log_S;
-        if (j >= a.nvec) continue;
-        uint32_t *base = gbase + j * a.col_stride + o;
-        const uint32_t *lbase = sgbase + j * scs + o;
-        uint32_t v[1 << K];
+        bool mine;
+        uint32_t *base;
+        if constexpr (PF) {
+            mine = have;
+            base = sb;
 #pragma unroll
-        for (int t = 0; t < (1 << K); ++t) v[t] = lbase[t * S];
+            for (int t = 0; t < NP; ++t) v[t] = nv[t];
+            have = u + 1 < u1 && locate(u + 1, lb, sb);
+            if (have) {
+#pragma unroll
+                for (int t = 0; t < NP; ++t) nv[t] = lb[t * S];
+            }
+        } else {
+            mine = locate(u, lb, sb);
+            base = sb;
+            if (mine) {
+#pragma unroll
+                for (int t = 0; t < (1 << K); ++t) v[t] = lb[t * S];
+            }
+        }
+        if (!mine) continue;
         pencil_stages<K, 0, INV>(v, smraw, 0, 0);
-        // recompute the store addresses instead of keeping 2^K pointers live
-        uint64_t S2;
-        asm volatile("mov.b64 %0, %1;" : "=l"(S2) : "l"(S));
-        uint32_t *base2;
-        asm volatile("mov.b64 %0, %1;" : "=l"(base2) : "l"(base));
+        if constexpr (!PF) {
+            // recompute the store addresses instead of keeping 2^K pointers live
+            uint64_t S2;
+            asm volatile("mov.b64 %0, %1;" : "=l"(S2) : "l"(S));
+            asm volatile("mov.b64 %0, %1;" : "=l"(base) : "l"(base));
 #pragma unroll
-        for (int t = 0; t < (1 << K); ++t) base2[t * S2] = v[t];
+            for (int t = 0; t < (1 << K); ++t) base[t * S2] = v[t];
+        } else {
+#pragma unroll
+            for (int t = 0; t < (1 << K); ++t) base[t * S] = v[t];
+        }
     }
 }
 
