@@ -153,11 +153,16 @@ const uint32_t *get_fft_tw(lg_ctx *c, uint32_t log_n) {
 // Per-call scratch: small device buffers come from a bump arena, uploads
 // and downloads go through a pinned bump arena without synchronising, and
 // host-side results of downloads (openings) are materialised by finalizers
-// after the call's last synchronisation.
+// after the call's last synchronisation.  Deferred downloads (of arena
+// buffers, which live until the call ends) are only queued by flush(), so
+// that the kernels between them run back to back and the copies go out
+// while the host has other work.
 struct Scratch {
     lg_ctx *c;
     std::vector<DBuf> dev_overflow;
     std::vector<std::function<void()>> finalizers;
+    struct Deferred { uint8_t *h; const void *d; size_t bytes; };
+    std::vector<Deferred> deferred;
     explicit Scratch(lg_ctx *ctx) : c(ctx) {
         constexpr size_t kPin = 8u << 20, kDev = 32u << 20;
         if (!c->pin_arena) {
@@ -171,8 +176,13 @@ struct Scratch {
         c->pin_used = 0;
         c->dev_used = 0;
     }
+    void flush() {
+        for (auto &x : deferred) CK(c, cudaMemcpyAsync(x.h, x.d, x.bytes, cudaMemcpyDeviceToHost, c->stream));
+        deferred.clear();
+    }
     // all pending transfers done, then hand the host copies over
     void finish() {
+        flush();
         sync(c);
         for (auto &f : finalizers) f();
         finalizers.clear();
@@ -218,6 +228,13 @@ struct Scratch {
         const size_t bytes = count * sizeof(T);
         uint8_t *h = pin(bytes);
         CK(c, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+        return reinterpret_cast<const T *>(h);
+    }
+    template <class T>
+    const T *download_deferred(const T *d, size_t count) {  // valid after finish()
+        const size_t bytes = count * sizeof(T);
+        uint8_t *h = pin(bytes);
+        deferred.push_back({h, d, bytes});
         return reinterpret_cast<const T *>(h);
     }
 };
@@ -344,6 +361,26 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
     return w;
 }
 
+// The same opening from host copies of the matrix (column-major, rows x
+// cols) and of the tree (all layers, leaves first, 32 bytes per node).
+void open_rows_host(const uint32_t *E, const uint8_t *tree, uint64_t rows, uint32_t cols,
+                    const std::vector<uint64_t> &q, lg::Opening *out) {
+    out->rows.resize(q.size());
+    for (size_t k = 0; k < q.size(); ++k) {
+        out->rows[k].resize(cols);
+        for (uint32_t j = 0; j < cols; ++j) out->rows[k][j] = E[(uint64_t)j * rows + q[k]];
+    }
+    std::vector<NodeRef> refs;
+    lg::merkle_proof_nodes(q, rows, refs);
+    uint64_t layer_off[64] = {0};
+    for (uint32_t l = 1; l < 64; ++l) layer_off[l] = layer_off[l - 1] + (rows >> (l - 1));
+    out->merkle.resize(refs.size());
+    for (size_t i = 0; i < refs.size(); ++i) {
+        const uint8_t *b = tree + 32 * (layer_off[refs[i].layer] + refs[i].index);
+        out->merkle[i].assign(b, b + 32);
+    }
+}
+
 // extract_row for each query (src/ligero.rs:40-51) + merkle_tree::prove
 // (src/merkle_tree.rs:98-111): device gathers, host copies materialised
 // into `out` at sc.finish().  Returns the device copy of the opened rows
@@ -383,7 +420,8 @@ std::pair<const uint32_t *, const uint64_t *> open_rows(lg_ctx *c, Scratch &sc, 
 // and of the queries.
 std::pair<const uint32_t *, const uint64_t *> open_rows_dev(lg_ctx *c, Scratch &sc, const Witness &w,
                                                             lgk::FsState *fs, const uint32_t *absorb, uint32_t nsq,
-                                                            uint32_t *out, lg::Opening *op) {
+                                                            uint32_t *out, lg::Opening *op,
+                                                            uint32_t *absorb_mirror = nullptr) {
     const uint32_t nq = LG_NUM_QUERIES;
     uint32_t depth = 0;
     while ((1ull << depth) < w.rows) ++depth;
@@ -403,10 +441,11 @@ std::pair<const uint32_t *, const uint64_t *> open_rows_dev(lg_ctx *c, Scratch &
     a.nnodes = d_cnt;
     a.nsq = nsq;
     a.out = out;
+    a.mirror = absorb_mirror;
     CK(c, lgk::fs_queries(c->L, fs, a));
     CK(c, lgk::gather_rows(c->L, w.E.u32(), w.rows, w.cols, d_q, nq, d_out));
     CK(c, lgk::gather_nodes(c->L, w.tree.u32(), d_nodes, cap, d_out + nq * w.cols, d_cnt));
-    const uint32_t *h = sc.download_later(d_out, nq * w.cols + (size_t)cap * 8 + 1);
+    const uint32_t *h = sc.download_deferred(d_out, nq * w.cols + (size_t)cap * 8 + 1);
     const uint32_t cols = w.cols;
     sc.finalizers.push_back([h, nq, cap, cols, op]() {
         op->rows.resize(nq);
@@ -507,12 +546,17 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
     auto next_tri = [&]() { return tri + 4 * ntri_used++; };
     CK(c, cudaMemsetAsync(tri, 0, 16ull * ntri + 16, c->stream));
     CK(c, lgk::fs_init(c->L, fs, LG_FS_SEED));
-    auto root_later = [&](const Witness &w, std::vector<uint8_t> *dst) {
-        const uint32_t *h = sc.download_later(w.root(), 8);
+    // A root reaches the host from the arena copy that the transcript
+    // kernel absorbing it writes (the tree itself may be freed before the
+    // deferred copies are queued).
+    auto root_later = [&](std::vector<uint8_t> *dst) {
+        uint32_t *mirror = static_cast<uint32_t *>(sc.dev(32));
+        const uint32_t *h = sc.download_deferred(mirror, 8);
         sc.finalizers.push_back([h, dst]() {
             const uint8_t *b = reinterpret_cast<const uint8_t *>(h);
             dst->assign(b, b + 32);
         });
+        return mirror;
     };
     auto tail = [&](bool check, uint32_t nsq, uint32_t *out) {
         lgk::FsTail a;
@@ -523,8 +567,10 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
         a.out = out;
         return a;
     };
-    auto step = [&](const uint32_t *src, uint32_t nwords, bool check, uint32_t nsq, uint32_t *out) {
+    auto step = [&](const uint32_t *src, uint32_t nwords, bool check, uint32_t nsq, uint32_t *out,
+                    uint32_t *mirror) {
         lgk::FsStep a;
+        a.mirror = mirror;
         a.src = src;
         a.nwords = nwords;
         a.check = check;
@@ -536,19 +582,19 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
     Witness w0 = h_poly ? commit_from_host(c, sc, h_poly, const_cast<uint32_t *>(d_poly), cfg.initial_log_m,
                                            1u << cfg.initial_log_n)
                         : commit(c, d_poly, cfg.initial_log_m, 1u << cfg.initial_log_n);  // :32-37
-    root_later(w0, &P.initial_root);
+    uint32_t *root_m = root_later(&P.initial_root);
     P.recursive_roots.resize(steps);
     P.recursive.resize(steps - 1);  // openings are filled in by pointer later
     const uint32_t *pe0 = next_chal(cfg.initial_k);
-    step(w0.root(), 8, false, cfg.initial_k, const_cast<uint32_t *>(pe0));  // :48-50
+    step(w0.root(), 8, false, cfg.initial_k, const_cast<uint32_t *>(pe0), root_m);  // :48-50
     uint32_t fv = cfg.initial_log_m;  // log2 |f|
     DBuf f(c, 4ull << fv);
     partial_eval_dev(c, d_poly, cfg.initial_log_m + cfg.initial_log_n, nullptr, cfg.initial_k, f.u32(), pe0);  // :52-53
 
     Witness wprev = commit(c, f.u32(), cfg.log_m[0], 1u << cfg.log_n[0]);  // :55-60
-    root_later(wprev, &P.recursive_roots[0]);
+    root_m = root_later(&P.recursive_roots[0]);
     uint32_t *alpha = next_chal(1);
-    auto opened = open_rows_dev(c, sc, w0, fs, wprev.root(), 1, alpha, &P.initial);  // :64-76
+    auto opened = open_rows_dev(c, sc, w0, fs, wprev.root(), 1, alpha, &P.initial, root_m);  // :64-76
     DBuf B(c, 4ull << fv);
     uint32_t *t = next_tri();
     induce_dev(c, sc, fv, opened.first, LG_NUM_QUERIES, nullptr, cfg.initial_k, opened.second, 0, B.u32(), t + 3, pe0,
@@ -564,6 +610,24 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
     DBuf f2(c, 4ull << (fv - 1)), B2(c, 4ull << (fv - 1));
     for (uint32_t i = 0; i < steps; ++i) {
         const uint32_t *rs = r;  // this step's ks[i] round challenges are consecutive
+        // The last commitment is final here: a side stream brings its matrix
+        // and tree to the host during this step's rounds, so the final
+        // opening needs no second round trip (when they are small and the
+        // pinned arena has room for them and the last downloads).
+        const uint32_t *h_E = nullptr;
+        const uint8_t *h_tree = nullptr;
+        const size_t eb = 4ull * wprev.rows * wprev.cols, tb = 32ull * (2 * wprev.rows - 1);
+        if (i == steps - 1 && eb + tb <= (4u << 20) &&
+            c->pin_used + eb + tb + (4ull << fv) + (1u << 16) <= c->pin_cap) {
+            uint8_t *h = sc.pin(eb + tb);
+            h_E = reinterpret_cast<const uint32_t *>(h);
+            h_tree = h + eb;
+            CK(c, cudaEventRecord(c->copy_ev[6], c->stream));
+            CK(c, cudaStreamWaitEvent(c->copy_stream, c->copy_ev[6], 0));
+            CK(c, cudaMemcpyAsync(h, wprev.E.p, eb, cudaMemcpyDeviceToHost, c->copy_stream));
+            CK(c, cudaMemcpyAsync(h + eb, wprev.tree.p, tb, cudaMemcpyDeviceToHost, c->copy_stream));
+            CK(c, cudaEventRecord(c->copy_ev[6], c->copy_stream));
+        }
         for (uint32_t k = 0; k < cfg.ks[i]; ++k) {  // :97-102
             t = next_tri();
             const bool more = k + 1 < cfg.ks[i];
@@ -580,7 +644,11 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
             const uint32_t *hy = sc.download_later(f.u32(), 1ull << fv);
             const lgk::FsState *hs = sc.download_later(fs, 1);
             const uint32_t *ht = sc.download_later(tri, 4ull * ntri);
-            sc.finish();
+            if (h_E) CK(c, cudaStreamWaitEvent(c->stream, c->copy_ev[6], 0));
+            // wait for these three only; the deferred downloads (roots,
+            // openings) go out now, while the host finishes the transcript
+            sync(c);
+            sc.flush();
             std::memcpy(P.yr.data(), hy, 4ull << fv);
             for (uint32_t j = 0; j < ntri; ++j) P.transcript.push_back({ht[4 * j], ht[4 * j + 1], ht[4 * j + 2]});
             if (hs->err) throw ProverAssert{};
@@ -594,13 +662,14 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
             fsh.absorb_u32s(P.yr.data(), P.yr.size());
             std::vector<uint64_t> q;
             if (!fsh.get_distinct_queries(wprev.rows, LG_NUM_QUERIES, q)) throw ProverAssert{};
-            open_rows(c, sc, wprev, q, &P.final_);
+            if (h_E) open_rows_host(h_E, h_tree, wprev.rows, wprev.cols, q, &P.final_);
+            else open_rows(c, sc, wprev, q, &P.final_);
             return;
         }
         Witness wn = commit(c, f.u32(), cfg.log_m[i + 1], 1u << cfg.log_n[i + 1]);  // :145-155
-        root_later(wn, &P.recursive_roots[i + 1]);
+        root_m = root_later(&P.recursive_roots[i + 1]);
         uint32_t *al = next_chal(1);
-        auto op = open_rows_dev(c, sc, wprev, fs, wn.root(), 1, al, &P.recursive[i]);  // :156-172
+        auto op = open_rows_dev(c, sc, wprev, fs, wn.root(), 1, al, &P.recursive[i], root_m);  // :156-172
         DBuf bi(c, 4ull << fv);
         t = next_tri();
         induce_dev(c, sc, fv, op.first, LG_NUM_QUERIES, nullptr, cfg.ks[i], op.second, 0, bi.u32(), t + 3, rs, al);
@@ -907,7 +976,7 @@ lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
         delete c;
         return LG_ERR_CUDA;
     }
-    if (cudaMalloc((void **)&c->L.dtab, lgk::kDtabWords * 4) != cudaSuccess) {
+    if (cudaMalloc((void **)&c->L.dtab, lgk::kDtabSlots * lgk::kDtabWords * 4) != cudaSuccess) {
         cudaGetLastError();
         cudaStreamDestroy(c->copy_stream);
         cudaStreamDestroy(c->stream);

@@ -50,7 +50,7 @@ __global__ void k_fs_step(FsState *g, FsStep a) {
     __shared__ uint32_t stage[32];
     load_state(S, g);
     const bool bad = threadIdx.x == 0 && a.check && (a.src[0] ^ a.src[1]) != a.src[3];
-    fs_absorb_block(S, a.src, a.nwords, stage, 32);
+    fs_absorb_block(S, a.src, a.nwords, stage, 32, a.mirror);
     if (bad) S.err |= FS_ERR_SUMCHECK;
     __syncthreads();
     fs_fields(S, B, a.nsq, a.out);
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a)
     __shared__ uint32_t take_sh, batch_sh;
     const uint32_t tid = threadIdx.x;
     load_state(S, g);
-    fs_absorb_block(S, a.src, a.nwords, lo32, kQBlock);
+    fs_absorb_block(S, a.src, a.nwords, lo32, kQBlock, a.mirror);
     const bool ok = a.n >= a.s && a.s >= 1 && a.s <= kQBlock;
     const uint64_t mask = a.n - 1;  // n is a power of two: % n is a mask
     uint32_t count = 0, batch = 0, take = 0;

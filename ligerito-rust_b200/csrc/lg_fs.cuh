@@ -73,11 +73,15 @@ __device__ void fs_absorb(FsState &S, const uint32_t *src, uint32_t nwords) {
 // The whole block absorbs nwords u32s from device memory: each run of up
 // to `cap` words is loaded in parallel into the shared `stage`, then
 // thread 0 absorbs it, so the words cost one memory round trip per run
-// instead of one each.
-__device__ void fs_absorb_block(FsState &S, const uint32_t *src, uint32_t nwords, uint32_t *stage, uint32_t cap) {
+// instead of one each.  A non-null mirror receives a copy of the words.
+__device__ void fs_absorb_block(FsState &S, const uint32_t *src, uint32_t nwords, uint32_t *stage, uint32_t cap,
+                                uint32_t *mirror) {
     for (uint32_t base = 0; base < nwords; base += cap) {
         const uint32_t n = min(cap, nwords - base);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) stage[i] = src[base + i];
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            stage[i] = src[base + i];
+            if (mirror) mirror[base + i] = stage[i];
+        }
         __syncthreads();
         if (threadIdx.x == 0) fs_absorb(S, stage, n);
         __syncthreads();

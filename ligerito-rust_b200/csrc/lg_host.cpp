@@ -211,11 +211,19 @@ std::array<uint64_t, 2> Transcript::squeeze() {
 bool Transcript::get_distinct_queries(uint64_t n, size_t s, std::vector<uint64_t> &out) {
     out.clear();
     if (n < s || n == 0) return false;
-    std::unordered_set<uint64_t> seen;
-    seen.reserve(2 * s);
+    // values seen so far: open addressing over at least 4s slots; ~0 marks
+    // an empty slot and is never a query (queries are < n)
+    size_t cap = 64;
+    while (cap < 4 * s) cap <<= 1;
+    std::vector<uint64_t> seen(cap, ~0ull);
     while (out.size() < s) {
-        uint64_t q = get_query(n);
-        if (seen.insert(q).second) out.push_back(q);
+        const uint64_t q = get_query(n);
+        size_t h = (size_t)((q * 0x9E3779B97F4A7C15ull) >> 40) & (cap - 1);
+        while (seen[h] != ~0ull && seen[h] != q) h = (h + 1) & (cap - 1);
+        if (seen[h] == ~0ull) {
+            seen[h] = q;
+            out.push_back(q);
+        }
     }
     std::sort(out.begin(), out.end());
     return true;

@@ -93,8 +93,50 @@ __global__ void k_rs_scale(const uint32_t *__restrict__ poly, const uint32_t *__
         out[idx] = gf_mul(poly[idx], pis[idx & (m - 1)]);
 }
 
+// The same scaling for many columns: every column multiplies row i by the
+// same pis[i], so a block takes 32 rows x up to 64 columns, builds the 32
+// rows' multiplication tables and multiplies with table lookups that every
+// lane of a warp shares.  The tile goes through shared memory with an odd
+// column stride: rows along lanes for the coalesced global accesses,
+// columns along lanes for the lookups, both free of bank conflicts.
+constexpr uint32_t kScaleRows = 32, kScaleCols = 64;
+__global__ void __launch_bounds__(256) k_rs_scale_tab(const uint32_t *__restrict__ poly,
+                                                      const uint32_t *__restrict__ pis, uint32_t *__restrict__ out,
+                                                      uint32_t log_m, uint32_t n) {
+    pdl_begin();
+    __shared__ __align__(512) uint32_t tabs[kScaleRows][kTabWords];
+    __shared__ uint32_t tile[kScaleCols * (kScaleRows + 1)];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t m = 1ull << log_m;
+    const uint64_t i0 = (uint64_t)blockIdx.x * kScaleRows;
+    const uint32_t j0 = blockIdx.y * kScaleCols, ncol = min(kScaleCols, n - j0);
+    for (uint32_t r = warp; r < kScaleRows; r += blockDim.x >> 5) tab_build_warp(tabs[r], __ldg(pis + i0 + r), lane);
+    for (uint32_t c = threadIdx.x; c < ncol * kScaleRows; c += blockDim.x) {
+        const uint32_t j = c / kScaleRows, r = c % kScaleRows;
+        tile[j * (kScaleRows + 1) + r] = __ldg(poly + (uint64_t)(j0 + j) * m + i0 + r);
+    }
+    __syncthreads();
+    for (uint32_t r = warp; r < kScaleRows; r += blockDim.x >> 5)
+        for (uint32_t j = lane; j < ncol; j += 32) {
+            uint32_t *x = tile + j * (kScaleRows + 1) + r;
+            *x = tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * r, 0, *x);
+        }
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < ncol * kScaleRows; c += blockDim.x) {
+        const uint32_t j = c / kScaleRows, r = c % kScaleRows;
+        out[(uint64_t)(j0 + j) * m + i0 + r] = tile[j * (kScaleRows + 1) + r];
+    }
+}
+
 cudaError_t rs_scale(Launcher &L, const uint32_t *poly, const uint32_t *pis, uint32_t *out, uint32_t log_m,
                      uint32_t n) {
+    if (n >= kScaleCols / 2 && log_m >= 5) {
+        // a table costs about as much as 30 general products: worth it from
+        // 32 columns on
+        const dim3 grid((unsigned)((1ull << log_m) / kScaleRows), (n + kScaleCols - 1) / kScaleCols);
+        LGK_LAUNCH(L, "rs_scale", launch_k(k_rs_scale_tab, grid, 256, 0, L.stream, poly, pis, out, log_m, n));
+        return cudaGetLastError();
+    }
     const uint64_t total = (uint64_t)n << log_m;
     const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
     LGK_LAUNCH(L, "rs_scale", launch_k(k_rs_scale, blocks, 256, 0, L.stream, poly, pis, out, log_m, total));
@@ -468,14 +510,22 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
     // D tables of every pass; kept while the same twiddle subtree is asked
     // for again (the twiddle arrays live, unchanged, as long as the context)
     const Launcher::DtabKey key{tw, log_len, root_base};
-    if (!(L.dtab_key == key)) {
+    uint32_t slot = 0;
+    while (slot < kDtabSlots && !(L.dtab_key[slot] == key)) ++slot;
+    if (slot == kDtabSlots) {
+        slot = 0;
+        for (uint32_t i = 1; i < kDtabSlots; ++i)
+            if (L.dtab_used[i] < L.dtab_used[slot]) slot = i;
         DtabArgs d{};
         for (uint32_t p = 0; p < np; ++p) { d.l0[p] = lr + d0s[p]; d.K[p] = ks[p]; }
-        LGK_LAUNCH(L, "fft_dtab", launch_k(k_fft_dtab, dim3(8, np), 256, 0, L.stream, tw, d, L.dtab));
+        LGK_LAUNCH(L, "fft_dtab",
+                   launch_k(k_fft_dtab, dim3(8, np), 256, 0, L.stream, tw, d, L.dtab + slot * kDtabWords));
         cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) { L.dtab_key = {}; return e; }
-        L.dtab_key = key;
+        if (e != cudaSuccess) { L.dtab_key[slot] = {}; return e; }
+        L.dtab_key[slot] = key;
     }
+    L.dtab_used[slot] = ++L.dtab_clock;
+    const uint32_t *dtab = L.dtab + slot * kDtabWords;
     uint32_t nvec_p2 = 1;
     while (nvec_p2 < nvec) nvec_p2 <<= 1;
     const bool aligned = ((uintptr_t)data % 16 == 0) && (col_stride % 4 == 0) && (q_stride % 4 == 0);
@@ -485,7 +535,7 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
         const uint32_t K = ks[p], d0 = d0s[p];
         PassArgs a;
         a.data = data; a.tw = tw; a.col_stride = col_stride; a.q_stride = q_stride;
-        a.dtab = reinterpret_cast<const uint4 *>(L.dtab + (size_t)p * 63 * kTabWords);
+        a.dtab = reinterpret_cast<const uint4 *>(dtab + (size_t)p * 63 * kTabWords);
         a.src = (src && p == 0) ? src->p : nullptr;
         a.src_col_stride = src ? src->col_stride : 0;
         a.src_q_stride = src ? src->q_stride : 0;
@@ -902,7 +952,7 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
 // the whole Lo_k vector by it.
 InducePlan induce_plan(uint32_t n, uint32_t nq) {
     InducePlan p;
-    p.b = std::min<uint32_t>(n, 10);
+    p.b = std::min<uint32_t>(n, 9);
     const uint64_t blocks_t = 1ull << (n - p.b);
     uint32_t qs = 1;
     while (blocks_t * qs < 3 * 296 && qs * 16 < nq) qs *= 2;  // about 3 waves of 2 blocks per SM

@@ -16,18 +16,23 @@ namespace lgk {
 // pass has at most 63 node tables of 128 words.
 constexpr uint32_t kMaxFftPasses = 6;
 constexpr size_t kDtabWords = kMaxFftPasses * 63 * 128;
+// D-table sets kept per context: one per FFT size a proof uses (its
+// commitments), so a steady run of proofs builds none
+constexpr uint32_t kDtabSlots = 4;
 
 struct Launcher {
     cudaStream_t stream = nullptr;
-    // device scratch of kDtabWords, owned by the context: the FFT passes'
-    // shared twiddle tables (fft_vectors), reused in stream order, and the
-    // twiddle subtree they were built for
+    // device scratch of kDtabSlots x kDtabWords, owned by the context: sets
+    // of the FFT passes' shared twiddle tables (fft_vectors), rebuilt in
+    // stream order, each with the twiddle subtree it was built for and its
+    // last use (the least recently used set is rebuilt first)
     uint32_t *dtab = nullptr;
     struct DtabKey {
         const uint32_t *tw = nullptr;
         uint32_t log_len = 0, root_base = 0;
         bool operator==(const DtabKey &o) const { return tw == o.tw && log_len == o.log_len && root_base == o.root_base; }
-    } dtab_key;
+    } dtab_key[kDtabSlots];
+    uint64_t dtab_used[kDtabSlots] = {}, dtab_clock = 0;
     uint64_t launches = 0;
     bool timing = false;
     struct Pending { std::string name; cudaEvent_t a, b; };
@@ -211,6 +216,7 @@ struct FsStep {
     uint32_t nwords = 0, check = 0;
     uint32_t nsq = 0;
     uint32_t *out = nullptr;
+    uint32_t *mirror = nullptr;  // when set, also receives the absorbed words
 };
 cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a);
 // Absorb nwords u32s of src; get_distinct_queries(n, s) sorted into q
@@ -229,6 +235,7 @@ struct FsQueries {
     uint32_t *nnodes = nullptr;
     uint32_t nsq = 0;
     uint32_t *out = nullptr;
+    uint32_t *mirror = nullptr;  // when set, also receives the absorbed words
 };
 cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a);
 

@@ -61,7 +61,7 @@ def test_fft_microbench_sizes_roundtrip(lg, ref, ctx, log_n, batch):
     assert torch.equal(d, keep)
 
 
-@pytest.mark.parametrize("log_m,n", [(6, 1), (6, 4), (6, 16), (8, 64), (10, 16), (11, 3), (12, 64), (14, 16)])
+@pytest.mark.parametrize("log_m,n", [(6, 1), (6, 4), (6, 16), (8, 64), (10, 16), (11, 3), (12, 64), (14, 16), (7, 40), (9, 100)])
 def test_encode_and_commit_match_oracle(lg, ref, ctx, log_m, n):
     # encode_cols + extract_leaves + build_merkle_tree (src/ligero.rs:11-95)
     poly = rand_u32(n << log_m)
