@@ -747,9 +747,12 @@ __global__ void __launch_bounds__(128) k_merkle_warp(uint32_t *__restrict__ tree
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
     if (num_leaves == 0 || (num_leaves & (num_leaves - 1))) return cudaErrorInvalidValue;
     uint64_t off = 0, n = num_leaves;
+    // Three layers per launch with a thread per 8 nodes while a layer has
+    // 2^12 nodes or more (a warp climbing six layers leaves most of its
+    // lanes idle after the first); the last few layers, six per warp.
     while (n > 1) {
         cudaError_t e;
-        if (n >= (1ull << 18)) {
+        if (n >= (1ull << 12)) {
             const uint64_t threads = n / 8;
             LGK_LAUNCH(L, "merkle_thread3", launch_k(k_merkle_thread3, (unsigned)((threads + 127) / 128), 128, 0,
                                                      L.stream, tree, off, n, 1u));
