@@ -374,11 +374,11 @@ void open_rows_host(const uint32_t *E, const uint8_t *tree, uint64_t rows, uint3
     lg::merkle_proof_nodes(q, rows, refs);
     uint64_t layer_off[64] = {0};
     for (uint32_t l = 1; l < 64; ++l) layer_off[l] = layer_off[l - 1] + (rows >> (l - 1));
-    out->merkle.resize(refs.size());
-    for (size_t i = 0; i < refs.size(); ++i) {
-        const uint8_t *b = tree + 32 * (layer_off[refs[i].layer] + refs[i].index);
-        out->merkle[i].assign(b, b + 32);
-    }
+    out->merkle.data.resize(32 * refs.size());
+    for (size_t i = 0; i < refs.size(); ++i)
+        std::memcpy(out->merkle.data.data() + 32 * i, tree + 32 * (layer_off[refs[i].layer] + refs[i].index), 32);
+    out->merkle.off.resize(refs.size() + 1);
+    for (size_t i = 0; i <= refs.size(); ++i) out->merkle.off[i] = 32 * i;
 }
 
 // extract_row for each query (src/ligero.rs:40-51) + merkle_tree::prove
@@ -404,11 +404,7 @@ std::pair<const uint32_t *, const uint64_t *> open_rows(lg_ctx *c, Scratch &sc, 
     sc.finalizers.push_back([h, nq, nr, cols, out]() {
         out->rows.resize(nq);
         for (size_t k = 0; k < nq; ++k) out->rows[k].assign(h + k * cols, h + (k + 1) * cols);
-        out->merkle.resize(nr);
-        for (size_t i = 0; i < nr; ++i) {
-            const uint8_t *b = reinterpret_cast<const uint8_t *>(h + nq * cols + 8 * i);
-            out->merkle[i].assign(b, b + 32);
-        }
+        out->merkle.assign_fixed(reinterpret_cast<const uint8_t *>(h + nq * cols), nr, 32);
     });
     return {d_out, d_idx};
 }
@@ -451,11 +447,7 @@ std::pair<const uint32_t *, const uint64_t *> open_rows_dev(lg_ctx *c, Scratch &
         op->rows.resize(nq);
         for (size_t k = 0; k < nq; ++k) op->rows[k].assign(h + k * cols, h + (k + 1) * cols);
         const uint32_t nr = std::min(h[nq * cols + (size_t)cap * 8], cap);
-        op->merkle.resize(nr);
-        for (size_t i = 0; i < nr; ++i) {
-            const uint8_t *b = reinterpret_cast<const uint8_t *>(h + nq * cols + 8 * i);
-            op->merkle[i].assign(b, b + 32);
-        }
+        op->merkle.assign_fixed(reinterpret_cast<const uint8_t *>(h + nq * cols), nr, 32);
     });
     return {d_out, d_q};
 }
@@ -1241,8 +1233,8 @@ lg_status lg_merkle_verify(const uint8_t *root, const uint8_t *proof, uint64_t n
         return LG_ERR_INVALID_ARGUMENT;
     std::vector<std::array<uint8_t, 32>> layer(nq);
     for (uint64_t i = 0; i < nq; ++i) lg::blake3_hash(leaves + off[i], off[i + 1] - off[i], layer[i].data());
-    std::vector<std::vector<uint8_t>> sib(n_sib);
-    for (uint64_t i = 0; i < n_sib; ++i) sib[i].assign(proof + 32 * i, proof + 32 * i + 32);
+    lg::ByteList sib;
+    sib.assign_fixed(proof, n_sib, 32);
     bool good = false;
     if (!lg::merkle_verify(root, 32, sib, depth, layer, std::vector<uint64_t>(queries, queries + nq), &good)) {
         *ok = 0;

@@ -360,14 +360,29 @@ lg_status config_check(const lg_config &c, uint64_t poly_len) {
 namespace {
 struct Writer {
     std::vector<uint8_t> b;
-    void u32(uint32_t v) { for (int i = 0; i < 4; ++i) b.push_back((uint8_t)(v >> (8 * i))); }
-    void bytes(const std::vector<uint8_t> &v) { u32((uint32_t)v.size()); b.insert(b.end(), v.begin(), v.end()); }
-    void words(const std::vector<uint32_t> &v) { u32((uint32_t)v.size()); for (uint32_t x : v) u32(x); }
+    void raw(const void *p, size_t n) {
+        const size_t at = b.size();
+        b.resize(at + n);
+        if (n) std::memcpy(b.data() + at, p, n);
+    }
+    void u32(uint32_t v) {
+        const uint8_t x[4] = {(uint8_t)v, (uint8_t)(v >> 8), (uint8_t)(v >> 16), (uint8_t)(v >> 24)};
+        raw(x, 4);
+    }
+    void bytes(const uint8_t *p, size_t n) { u32((uint32_t)n); raw(p, n); }
+    void bytes(const std::vector<uint8_t> &v) { bytes(v.data(), v.size()); }
+    void words(const std::vector<uint32_t> &v) {
+        u32((uint32_t)v.size());
+        const size_t at = b.size();
+        b.resize(at + 4 * v.size());
+        uint8_t *d = b.data() + at;
+        for (uint32_t x : v) { d[0] = (uint8_t)x; d[1] = (uint8_t)(x >> 8); d[2] = (uint8_t)(x >> 16); d[3] = (uint8_t)(x >> 24); d += 4; }
+    }
     void opening(const Opening &o) {
         u32((uint32_t)o.rows.size());
         for (auto &r : o.rows) words(r);
         u32((uint32_t)o.merkle.size());
-        for (auto &s : o.merkle) bytes(s);
+        for (size_t i = 0; i < o.merkle.size(); ++i) bytes(o.merkle.ptr(i), o.merkle.len(i));
     }
 };
 struct Reader {
@@ -398,15 +413,21 @@ struct Reader {
         for (auto &row : o.rows) words(row);
         uint32_t s = u32();
         if (!count(s, 4)) return;
-        o.merkle.resize(s);
-        for (auto &x : o.merkle) bytes(x);
+        o.merkle.clear();
+        o.merkle.off.reserve(s + 1);
+        for (uint32_t i = 0; i < s && !bad; ++i) {
+            const uint32_t c = u32();
+            if (!count(c, 1)) return;
+            o.merkle.push(p + at, c);
+            at += c;
+        }
     }
 };
 }  // namespace
 
 std::vector<uint8_t> serialize(const Proof &p) {
     Writer w;
-    w.b.reserve(4096);
+    w.b.reserve(proof_size(p) + 4096);
     w.b.insert(w.b.end(), {'L', 'G', 'R', 'P'});
     w.u32(1);
     w.u32(4);
@@ -451,7 +472,7 @@ uint64_t proof_size(const Proof &p) {
     auto op = [](const Opening &o) {
         uint64_t s = 0;
         for (auto &r : o.rows) s += 4 * r.size();
-        for (auto &m : o.merkle) s += m.size();
+        s += o.merkle.data.size();
         return s;
     };
     uint64_t s = p.initial_root.size() + op(p.initial) + op(p.final_) + 4 * p.yr.size() +
@@ -495,7 +516,7 @@ static void hash_two(const uint8_t *l, const uint8_t *r, size_t rl_len, bool swa
 
 // verify_ith_layer (src/merkle_tree.rs:120-162) + verify (:164-188)
 bool merkle_verify(const uint8_t *root, size_t root_len,
-                   const std::vector<std::vector<uint8_t>> &proof, size_t depth,
+                   const ByteList &proof, size_t depth,
                    std::vector<std::array<uint8_t, 32>> layer, std::vector<uint64_t> q, bool *ok) {
     size_t cur = q.size(), pc = 0;
     *ok = false;
@@ -509,9 +530,9 @@ bool merkle_verify(const uint8_t *root, size_t root_len,
             if (i == cur - 1 || (query & 1) || q[i + 1] != sib) {
                 ++pc;
                 if (pc - 1 >= proof.size()) return false;  // index panic
-                const auto &s = proof[pc - 1];
-                if (s.size() > 1024) return false;
-                hash_two(layer[i].data(), s.data(), s.size(), (query & 1) != 0, h.data());
+                const size_t sl = proof.len(pc - 1);
+                if (sl > 1024) return false;
+                hash_two(layer[i].data(), proof.ptr(pc - 1), sl, (query & 1) != 0, h.data());
                 layer[next - 1] = h;
                 if (i == cur - 1) break;
                 i += 1;

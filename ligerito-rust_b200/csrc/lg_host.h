@@ -55,9 +55,30 @@ void blake3_hash(const uint8_t *msg, size_t len, uint8_t out[32]);
 lg_status config_check(const lg_config &c, uint64_t poly_len);
 
 // -------------------------------------------------------------------- proof
+// A list of byte strings (a Vec<Vec<u8>>) in one buffer: entry i is
+// data[off[i], off[i+1]).  Proofs hold thousands of 32-byte Merkle nodes;
+// one allocation for all of them instead of one each.
+struct ByteList {
+    std::vector<uint8_t> data;
+    std::vector<uint64_t> off = {0};
+    size_t size() const { return off.size() - 1; }
+    const uint8_t *ptr(size_t i) const { return data.data() + off[i]; }
+    size_t len(size_t i) const { return off[i + 1] - off[i]; }
+    void clear() { data.clear(); off.assign(1, 0); }
+    void push(const uint8_t *p, size_t n) {
+        data.insert(data.end(), p, p + n);
+        off.push_back(data.size());
+    }
+    // count entries of `each` bytes, back to back at p
+    void assign_fixed(const uint8_t *p, size_t count, size_t each) {
+        data.assign(p, p + count * each);
+        off.resize(count + 1);
+        for (size_t i = 0; i <= count; ++i) off[i] = i * each;
+    }
+};
 struct Opening {
-    std::vector<std::vector<uint32_t>> rows;   // opened_rows
-    std::vector<std::vector<uint8_t>> merkle;  // merkle_proof
+    std::vector<std::vector<uint32_t>> rows;  // opened_rows
+    ByteList merkle;                          // merkle_proof
 };
 struct Proof {  // FinalizedLigeritoProof, src/data_structures.rs:91-103
     std::vector<uint8_t> initial_root;
@@ -82,7 +103,7 @@ void merkle_proof_nodes(const std::vector<uint64_t> &queries, uint64_t num_leave
 // Returns false where the reference would panic (proof index out of range);
 // *ok receives the reference's bool otherwise.
 bool merkle_verify(const uint8_t *root, size_t root_len,
-                   const std::vector<std::vector<uint8_t>> &proof, size_t depth,
+                   const ByteList &proof, size_t depth,
                    std::vector<std::array<uint8_t, 32>> layer, std::vector<uint64_t> queries,
                    bool *ok);
 
