@@ -457,9 +457,9 @@ class FinalizedLigeritoProof:
     def to_bytes(self) -> bytes:
         n = ctypes.c_uint64()
         _check(lib.lg_proof_serialize(self.handle, None, ctypes.byref(n)))
-        buf = ctypes.create_string_buffer(n.value)
-        _check(lib.lg_proof_serialize(self.handle, buf, ctypes.byref(n)))
-        return buf.raw[: n.value]
+        out = bytearray(n.value)
+        _check(lib.lg_proof_serialize(self.handle, (ctypes.c_char * len(out)).from_buffer(out), ctypes.byref(n)))
+        return bytes(out)
 
     @classmethod
     def from_bytes(cls, b: bytes) -> "FinalizedLigeritoProof":

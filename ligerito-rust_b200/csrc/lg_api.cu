@@ -1080,9 +1080,13 @@ lg_status lg_verify(lg_ctx *c, const lg_config *cfg, const lg_proof *proof, int 
 
 lg_status lg_proof_serialize(const lg_proof *p, uint8_t *buf, uint64_t *len) {
     if (!p || !len) return LG_ERR_INVALID_ARGUMENT;
+    const size_t need = lg::serialized_size(p->p);
+    if (!buf || *len < need) {
+        const bool ask = !buf;
+        *len = need;
+        return ask ? LG_OK : LG_ERR_INVALID_ARGUMENT;
+    }
     std::vector<uint8_t> b = lg::serialize(p->p);
-    if (!buf) { *len = b.size(); return LG_OK; }
-    if (*len < b.size()) { *len = b.size(); return LG_ERR_INVALID_ARGUMENT; }
     std::memcpy(buf, b.data(), b.size());
     *len = b.size();
     return LG_OK;

@@ -425,9 +425,23 @@ struct Reader {
 };
 }  // namespace
 
+// Length of serialize(p), without building it
+size_t serialized_size(const Proof &p) {
+    auto op = [](const Opening &o) {
+        size_t s = 8 + 4 * o.merkle.size() + o.merkle.data.size();
+        for (auto &r : o.rows) s += 4 + 4 * r.size();
+        return s;
+    };
+    size_t s = 12 + 4 + p.initial_root.size() + 4 + op(p.initial) + 4 + 4 + 4 * p.yr.size() + op(p.final_) + 4 +
+               12 * p.transcript.size();
+    for (auto &r : p.recursive_roots) s += 4 + r.size();
+    for (auto &o : p.recursive) s += op(o);
+    return s;
+}
+
 std::vector<uint8_t> serialize(const Proof &p) {
     Writer w;
-    w.b.reserve(proof_size(p) + 4096);
+    w.b.reserve(serialized_size(p));
     w.b.insert(w.b.end(), {'L', 'G', 'R', 'P'});
     w.u32(1);
     w.u32(4);

@@ -90,6 +90,7 @@ struct Proof {  // FinalizedLigeritoProof, src/data_structures.rs:91-103
     std::vector<std::array<uint32_t, 3>> transcript;
 };
 std::vector<uint8_t> serialize(const Proof &p);
+size_t serialized_size(const Proof &p);
 bool deserialize(const uint8_t *buf, size_t len, Proof &p);
 uint64_t proof_size(const Proof &p);  // ProofSize, src/data_structures.rs:105-194
 
