@@ -816,20 +816,30 @@ __device__ __forceinline__ uint32_t lagrange_at(const uint32_t *rs, uint32_t k, 
     return p;
 }
 
+// NJ = 2^k values per output, loaded in runs of up to 8 independent loads
+// ahead of their products so that HBM latency overlaps.
+template <int NJ>
 __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-                                                 uint64_t M, uint32_t nj, Coeffs64 gr, const uint32_t *d_rs,
-                                                 uint32_t k) {
+                                                 uint64_t M, Coeffs64 gr, const uint32_t *d_rs, uint32_t k) {
     pdl_begin();
     extern __shared__ __align__(128) uint8_t tabs8[];
     __shared__ uint32_t g[64];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (threadIdx.x < nj) g[threadIdx.x] = d_rs ? lagrange_at(d_rs, k, threadIdx.x) : gr.v[threadIdx.x];
+    if (threadIdx.x < NJ) g[threadIdx.x] = d_rs ? lagrange_at(d_rs, k, threadIdx.x) : gr.v[threadIdx.x];
     __syncthreads();
-    for (uint32_t j = warp; j < nj; j += nw) tab_build_warp(reinterpret_cast<uint32_t *>(tabs8 + 512 * j), g[j], lane);
+    for (uint32_t j = warp; j < NJ; j += nw) tab_build_warp(reinterpret_cast<uint32_t *>(tabs8 + 512 * j), g[j], lane);
     __syncthreads();
+    constexpr int RUN = NJ < 8 ? NJ : 8;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t acc = 0;
-        for (uint32_t j = 0; j < nj; ++j) acc ^= tab_mul_sa(tabs8, 512u * j, 0, __ldg(in + j * M + i));
+#pragma unroll
+        for (int j0 = 0; j0 < NJ; j0 += RUN) {
+            uint32_t v[RUN];
+#pragma unroll
+            for (int u = 0; u < RUN; ++u) v[u] = __ldg(in + (uint64_t)(j0 + u) * M + i);
+#pragma unroll
+            for (int u = 0; u < RUN; ++u) acc ^= tab_mul_sa(tabs8, 512u * (j0 + u), 0, v[u]);
+        }
         out[i] = acc;
     }
 }
@@ -843,7 +853,13 @@ cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log
         for (uint32_t j = 0; j < nj; ++j) c.v[j] = gr[j];
     const uint64_t M = 1ull << (log_len - k);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((M + 255) / 256, 148ull * 8));
-    LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq, blocks, 256, nj * kTabWords * sizeof(uint32_t), L.stream, in, out, M, nj, c, d_rs, k));
+    const size_t smem = nj * kTabWords * sizeof(uint32_t);
+    switch (nj) {
+#define LGK_CASE(n) \
+    case n: LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<n>, blocks, 256, smem, L.stream, in, out, M, c, d_rs, k)); break;
+        LGK_CASE(2) LGK_CASE(4) LGK_CASE(8) LGK_CASE(16) LGK_CASE(32) LGK_CASE(64)
+#undef LGK_CASE
+    }
     return cudaGetLastError();
 }
 
