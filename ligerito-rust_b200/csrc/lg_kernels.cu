@@ -700,47 +700,65 @@ __global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ t
     }
 }
 
-// Narrow layers: a warp takes 2^lev consecutive nodes (lev <= 6) and climbs
-// lev layers, lane i of each layer hashing the pair its two source lanes
-// hold; one hash latency per layer.
-__global__ void __launch_bounds__(128) k_merkle_warp(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
-                                                     uint32_t lev, uint32_t one) {
+// Narrow layers: a block of 1024 threads takes 2048 consecutive nodes (or
+// the whole layer when it is smaller) and climbs to their common ancestor,
+// one layer per barrier: the first layer up reads the tree, the later ones
+// a shared-memory copy of the layer below.  Every node is also written to
+// the tree.  One launch takes a layer of up to 2^22 nodes eleven layers up
+// (a layer of 2048 or fewer nodes to the root).
+constexpr uint32_t kMerkleBlockNodes = 2048;
+__global__ void __launch_bounds__(1024) k_merkle_block(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
+                                                       uint32_t one) {
     pdl_begin();
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t per = 1ull << lev;
-    if (w * per >= n_in) return;  // whole warps only: n_in is a multiple of per
-    uint32_t h[8];
-    uint64_t off = in_off, n = n_in, first = w * per;  // first node of this warp in the layer
-    // first layer up: lane i < per/2 hashes nodes 2i, 2i+1 of the warp's run
-    {
-        uint32_t l[8], r[8];
-        const bool act = lane < per / 2;
-        if (act) {
-            load_node(tree + 8 * (off + first + 2 * lane), l);
-            load_node(tree + 8 * (off + first + 2 * lane + 1), r);
-            hash_pair(l, r, h, one);
-            store_node(tree + 8 * (off + n + first / 2 + lane), h);
-        }
-        off += n;
-        n >>= 1;
-        first >>= 1;
-    }
-    for (uint32_t k = 1; k < lev; ++k) {
-        const uint32_t cnt = (uint32_t)(per >> (k + 1));  // nodes made at this layer
-        uint32_t l[8], r[8];
+    // layers in shared memory word-major (word j of node i at [j * stride +
+    // i]): a thread reads its two children's word j as one 8-byte load and
+    // a warp's loads are contiguous
+    __shared__ __align__(16) uint32_t buf_a[8 * (kMerkleBlockNodes / 2)];
+    __shared__ __align__(16) uint32_t buf_b[8 * (kMerkleBlockNodes / 4)];
+    const uint32_t t = threadIdx.x;
+    uint32_t m = (uint32_t)(n_in < kMerkleBlockNodes ? n_in : kMerkleBlockNodes);  // this block's nodes in the layer
+    uint64_t off = in_off, n = n_in, first = blockIdx.x * (uint64_t)m;
+    if (t < m / 2) {
+        uint32_t l[8], r[8], h[8];
+        load_node(tree + 8 * (off + first + 2 * t), l);
+        load_node(tree + 8 * (off + first + 2 * t + 1), r);
+        hash_pair(l, r, h, one);
+        store_node(tree + 8 * (off + n + first / 2 + t), h);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            l[j] = __shfl_sync(0xffffffffu, h[j], (2 * lane) & 31);
-            r[j] = __shfl_sync(0xffffffffu, h[j], (2 * lane + 1) & 31);
-        }
-        if (lane < cnt) {
+        for (int j = 0; j < 8; ++j) buf_a[j * (kMerkleBlockNodes / 2) + t] = h[j];
+    }
+    off += n;
+    n >>= 1;
+    first >>= 1;
+    m >>= 1;
+    __syncthreads();
+    uint32_t *src = buf_a, *dst = buf_b;
+    uint32_t ss = kMerkleBlockNodes / 2, ds = kMerkleBlockNodes / 4;
+    while (m > 1) {
+        if (t < m / 2) {
+            uint32_t l[8], r[8], h[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const uint2 x = *reinterpret_cast<const uint2 *>(src + j * ss + 2 * t);
+                l[j] = x.x;
+                r[j] = x.y;
+            }
             hash_pair(l, r, h, one);
-            store_node(tree + 8 * (off + n + first / 2 + lane), h);
+            store_node(tree + 8 * (off + n + first / 2 + t), h);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) dst[j * ds + t] = h[j];
         }
         off += n;
         n >>= 1;
         first >>= 1;
+        m >>= 1;
+        __syncthreads();
+        uint32_t *tp = src;
+        src = dst;
+        dst = tp;
+        const uint32_t ts = ss;
+        ss = ds;
+        ds = ts;
     }
 }
 
@@ -748,23 +766,21 @@ cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
     if (num_leaves == 0 || (num_leaves & (num_leaves - 1))) return cudaErrorInvalidValue;
     uint64_t off = 0, n = num_leaves;
     // Three layers per launch with a thread per 8 nodes while a layer has
-    // 2^12 nodes or more (a warp climbing six layers leaves most of its
-    // lanes idle after the first); the last few layers, six per warp.
+    // 2^18 nodes or more (every lane does full work); narrower layers go up
+    // eleven at a time in blocks of 2048 nodes, a layer per barrier.
     while (n > 1) {
         cudaError_t e;
-        if (n >= (1ull << 12)) {
+        if (n >= (1ull << 18)) {
             const uint64_t threads = n / 8;
             LGK_LAUNCH(L, "merkle_thread3", launch_k(k_merkle_thread3, (unsigned)((threads + 127) / 128), 128, 0,
                                                      L.stream, tree, off, n, 1u));
             e = cudaGetLastError();
             for (int l = 0; l < 3; ++l) { off += n; n /= 2; }
         } else {
-            const uint32_t lev = std::min<uint32_t>(6, ilog2u(n));
-            const uint64_t warps = n >> lev;
-            LGK_LAUNCH(L, "merkle_warp", launch_k(k_merkle_warp, (unsigned)((warps * 32 + 127) / 128), 128, 0,
-                                                  L.stream, tree, off, n, lev, 1u));
+            const uint64_t per = std::min<uint64_t>(n, kMerkleBlockNodes);
+            LGK_LAUNCH(L, "merkle_block", launch_k(k_merkle_block, (unsigned)(n / per), 1024, 0, L.stream, tree, off, n, 1u));
             e = cudaGetLastError();
-            for (uint32_t l = 0; l < lev; ++l) { off += n; n /= 2; }
+            for (uint64_t m = per; m > 1; m /= 2) { off += n; n /= 2; }
         }
         if (e != cudaSuccess) return e;
     }
