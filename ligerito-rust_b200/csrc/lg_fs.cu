@@ -92,6 +92,31 @@ __device__ uint32_t hash_insert(unsigned long long *key, uint32_t *rank, uint64_
     return kHash - 1;  // unreachable: the table is never more than half full
 }
 
+// The chain of a batch (see fs_chain) from schedules prepared by the block:
+// thread t < full writes K + W of chain block t to kw[t], then thread 0
+// runs only the rounds.  The whole block calls it.
+__device__ void fs_chain_block(const FsState &S, Batch &B, uint32_t cnt, uint32_t (*kw)[64]) {
+    const uint32_t full = (S.nw + cnt) / 16;
+    if (threadIdx.x < full) {
+        uint32_t blk[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) blk[k] = stream_word(S, 16 * threadIdx.x + k);
+        sha_schedule_kw(blk, kw[threadIdx.x]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t st[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) B.chain[0][k] = st[k] = S.h[k];
+        for (uint32_t f = 0; f < full; ++f) {
+            sha_rounds_kw(st, kw[f]);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) B.chain[f + 1][k] = st[k];
+        }
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a) {
     pdl_begin();
     __shared__ FsState S;
@@ -103,6 +128,7 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a)
     __shared__ uint32_t scratch[kQBlock / 32];
     __shared__ uint32_t wcnt[64][kQBlock / 32];
     __shared__ uint32_t take_sh, batch_sh;
+    __shared__ uint32_t kw[kMaxChain][64];
     const uint32_t tid = threadIdx.x;
     load_state(S, g);
     fs_absorb_block(S, a.src, a.nwords, lo32, kQBlock, a.mirror);
@@ -117,8 +143,7 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a)
         // is its serial part
         const uint32_t need = a.s - count;
         batch = min(kQBlock, need + need / 16 + 8 + a.nsq);
-        if (tid == 0) fs_chain(S, B, batch);
-        __syncthreads();
+        fs_chain_block(S, B, batch, kw);
         uint64_t qv = 0;
         if (tid < batch) {
             const uint64_t lo = fs_squeeze_at(S, B, tid);

@@ -55,6 +55,41 @@ __device__ __forceinline__ void sha_compress(uint32_t st[8], const uint32_t (&bl
     st[0] += a; st[1] += b; st[2] += c; st[3] += d; st[4] += e; st[5] += f; st[6] += g; st[7] += h;
 }
 
+// The 64 rounds of a compression whose K[t] + W[t] are already in kw (the
+// message schedule computed elsewhere): the serial part alone.
+__device__ __forceinline__ void sha_rounds_kw(uint32_t st[8], const uint32_t *kw) {
+    uint32_t a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
+#pragma unroll 1
+    for (int t0 = 0; t0 < 64; t0 += 16) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const uint32_t hk = h + kw[t0 + i];
+            const uint32_t t1 = hk + (rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)) + ((e & f) ^ (~e & g));
+            const uint32_t t2 = (rr(a, 2) ^ rr(a, 13) ^ rr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+            h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+        }
+    }
+    st[0] += a; st[1] += b; st[2] += c; st[3] += d; st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+}
+
+// K[t] + W[t] (t < 64) of a block of 16 big-endian words.
+__device__ __forceinline__ void sha_schedule_kw(const uint32_t (&blk)[16], uint32_t *kw) {
+    uint32_t w[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) w[i] = blk[i];
+#pragma unroll 1
+    for (int t0 = 0; t0 < 64; t0 += 16) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            if (t0 > 0) {
+                const uint32_t x = w[(i + 1) & 15], y = w[(i + 14) & 15];
+                w[i] += (rr(x, 7) ^ rr(x, 18) ^ (x >> 3)) + w[(i + 9) & 15] + (rr(y, 17) ^ rr(y, 19) ^ (y >> 10));
+            }
+            kw[t0 + i] = kK256[t0 + i] + w[i];
+        }
+    }
+}
+
 // Serial absorb of nwords u32s (their LE bytes) by one thread.
 __device__ void fs_absorb(FsState &S, const uint32_t *src, uint32_t nwords) {
     for (uint32_t i = 0; i < nwords; ++i) {
