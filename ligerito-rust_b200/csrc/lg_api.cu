@@ -365,11 +365,11 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
 // cols) and of the tree (all layers, leaves first, 32 bytes per node).
 void open_rows_host(const uint32_t *E, const uint8_t *tree, uint64_t rows, uint32_t cols,
                     const std::vector<uint64_t> &q, lg::Opening *out) {
-    out->rows.resize(q.size());
-    for (size_t k = 0; k < q.size(); ++k) {
-        out->rows[k].resize(cols);
-        for (uint32_t j = 0; j < cols; ++j) out->rows[k][j] = E[(uint64_t)j * rows + q[k]];
-    }
+    out->rows.data.resize(q.size() * cols);
+    for (size_t k = 0; k < q.size(); ++k)
+        for (uint32_t j = 0; j < cols; ++j) out->rows.data[k * cols + j] = E[(uint64_t)j * rows + q[k]];
+    out->rows.off.resize(q.size() + 1);
+    for (size_t k = 0; k <= q.size(); ++k) out->rows.off[k] = k * cols;
     std::vector<NodeRef> refs;
     lg::merkle_proof_nodes(q, rows, refs);
     uint64_t layer_off[64] = {0};
@@ -402,8 +402,7 @@ std::pair<const uint32_t *, const uint64_t *> open_rows(lg_ctx *c, Scratch &sc, 
     const uint32_t *h = sc.download_later(d_out, nq * w.cols + nr * 8);
     const uint32_t cols = w.cols;
     sc.finalizers.push_back([h, nq, nr, cols, out]() {
-        out->rows.resize(nq);
-        for (size_t k = 0; k < nq; ++k) out->rows[k].assign(h + k * cols, h + (k + 1) * cols);
+        out->rows.assign_fixed(h, nq, cols);
         out->merkle.assign_fixed(reinterpret_cast<const uint8_t *>(h + nq * cols), nr, 32);
     });
     return {d_out, d_idx};
@@ -444,8 +443,7 @@ std::pair<const uint32_t *, const uint64_t *> open_rows_dev(lg_ctx *c, Scratch &
     const uint32_t *h = sc.download_deferred(d_out, nq * w.cols + (size_t)cap * 8 + 1);
     const uint32_t cols = w.cols;
     sc.finalizers.push_back([h, nq, cap, cols, op]() {
-        op->rows.resize(nq);
-        for (size_t k = 0; k < nq; ++k) op->rows[k].assign(h + k * cols, h + (k + 1) * cols);
+        op->rows.assign_fixed(h, nq, cols);
         const uint32_t nr = std::min(h[nq * cols + (size_t)cap * 8], cap);
         op->merkle.assign_fixed(reinterpret_cast<const uint8_t *>(h + nq * cols), nr, 32);
     });
@@ -695,9 +693,9 @@ bool opening_ok(const std::vector<uint8_t> &root, const lg::Opening &o, size_t d
     std::vector<std::array<uint8_t, 32>> layer(q.size());
     std::vector<uint8_t> buf;
     for (size_t i = 0; i < q.size(); ++i) {
-        buf.resize(4 * o.rows[i].size());
-        for (size_t j = 0; j < o.rows[i].size(); ++j) {
-            uint32_t v = o.rows[i][j];
+        buf.resize(4 * o.rows.len(i));
+        for (size_t j = 0; j < o.rows.len(i); ++j) {
+            uint32_t v = o.rows.ptr(i)[j];
             buf[4 * j] = (uint8_t)v; buf[4 * j + 1] = (uint8_t)(v >> 8);
             buf[4 * j + 2] = (uint8_t)(v >> 16); buf[4 * j + 3] = (uint8_t)(v >> 24);
         }
@@ -712,8 +710,8 @@ std::vector<uint32_t> dense(const lg::Opening &o, size_t want_rows, size_t want_
     if (o.rows.size() != want_rows) throw VerifyPanic{};  // assert_eq (src/sumcheck_polys.rs:98)
     std::vector<uint32_t> r(want_rows * want_len);
     for (size_t k = 0; k < want_rows; ++k) {
-        if (o.rows[k].size() != want_len) throw VerifyPanic{};  // :97
-        std::copy(o.rows[k].begin(), o.rows[k].end(), r.begin() + k * want_len);
+        if (o.rows.len(k) != want_len) throw VerifyPanic{};  // :97
+        std::copy(o.rows.ptr(k), o.rows.ptr(k) + want_len, r.begin() + k * want_len);
     }
     return r;
 }
@@ -730,8 +728,8 @@ void ligero_verify_host(const std::vector<uint64_t> &q, const lg::Opening &o, co
     if (o.rows.size() > q.size()) throw VerifyPanic{};
     for (size_t i = 0; i < o.rows.size(); ++i) {
         uint32_t dot = 0;
-        const size_t zl = std::min(o.rows[i].size(), gr.size());
-        for (size_t j = 0; j < zl; ++j) dot ^= lg::gf_mul(o.rows[i][j], gr[j]);
+        const size_t zl = std::min(o.rows.len(i), gr.size());
+        for (size_t j = 0; j < zl; ++j) dot ^= lg::gf_mul(o.rows.ptr(i)[j], gr[j]);
         if (q[i] > 0xFFFFFFFFull) throw VerifyPanic{};
         sx[0] = (uint32_t)q[i];
         for (uint32_t t = 1; t < nv; ++t) sx[t] = lg::next_s(sx[t - 1], sks[t - 1]);

@@ -371,16 +371,20 @@ struct Writer {
     }
     void bytes(const uint8_t *p, size_t n) { u32((uint32_t)n); raw(p, n); }
     void bytes(const std::vector<uint8_t> &v) { bytes(v.data(), v.size()); }
-    void words(const std::vector<uint32_t> &v) {
-        u32((uint32_t)v.size());
+    void words(const uint32_t *v, size_t n) {
+        u32((uint32_t)n);
         const size_t at = b.size();
-        b.resize(at + 4 * v.size());
+        b.resize(at + 4 * n);
         uint8_t *d = b.data() + at;
-        for (uint32_t x : v) { d[0] = (uint8_t)x; d[1] = (uint8_t)(x >> 8); d[2] = (uint8_t)(x >> 16); d[3] = (uint8_t)(x >> 24); d += 4; }
+        for (size_t i = 0; i < n; ++i, d += 4) {
+            const uint32_t x = v[i];
+            d[0] = (uint8_t)x; d[1] = (uint8_t)(x >> 8); d[2] = (uint8_t)(x >> 16); d[3] = (uint8_t)(x >> 24);
+        }
     }
+    void words(const std::vector<uint32_t> &v) { words(v.data(), v.size()); }
     void opening(const Opening &o) {
         u32((uint32_t)o.rows.size());
-        for (auto &r : o.rows) words(r);
+        for (size_t i = 0; i < o.rows.size(); ++i) words(o.rows.ptr(i), o.rows.len(i));
         u32((uint32_t)o.merkle.size());
         for (size_t i = 0; i < o.merkle.size(); ++i) bytes(o.merkle.ptr(i), o.merkle.len(i));
     }
@@ -409,8 +413,13 @@ struct Reader {
     void opening(Opening &o) {
         uint32_t r = u32();
         if (!count(r, 4)) return;
-        o.rows.resize(r);
-        for (auto &row : o.rows) words(row);
+        o.rows.clear();
+        o.rows.off.reserve(r + 1);
+        std::vector<uint32_t> row;
+        for (uint32_t i = 0; i < r && !bad; ++i) {
+            words(row);
+            if (!bad) o.rows.push(row.data(), row.size());
+        }
         uint32_t s = u32();
         if (!count(s, 4)) return;
         o.merkle.clear();
@@ -429,7 +438,7 @@ struct Reader {
 size_t serialized_size(const Proof &p) {
     auto op = [](const Opening &o) {
         size_t s = 8 + 4 * o.merkle.size() + o.merkle.data.size();
-        for (auto &r : o.rows) s += 4 + 4 * r.size();
+        s += 4 * o.rows.size() + 4 * o.rows.data.size();
         return s;
     };
     size_t s = 12 + 4 + p.initial_root.size() + 4 + op(p.initial) + 4 + 4 + 4 * p.yr.size() + op(p.final_) + 4 +
@@ -485,7 +494,7 @@ bool deserialize(const uint8_t *buf, size_t len, Proof &p) {
 uint64_t proof_size(const Proof &p) {
     auto op = [](const Opening &o) {
         uint64_t s = 0;
-        for (auto &r : o.rows) s += 4 * r.size();
+        s += 4 * o.rows.data.size();
         s += o.merkle.data.size();
         return s;
     };

@@ -76,9 +76,29 @@ struct ByteList {
         for (size_t i = 0; i <= count; ++i) off[i] = i * each;
     }
 };
+// The same for a list of u32 rows (a Vec<Vec<u32>>): row i is
+// data[off[i], off[i+1]).
+struct WordList {
+    std::vector<uint32_t> data;
+    std::vector<uint64_t> off = {0};
+    size_t size() const { return off.size() - 1; }
+    const uint32_t *ptr(size_t i) const { return data.data() + off[i]; }
+    size_t len(size_t i) const { return off[i + 1] - off[i]; }
+    void clear() { data.clear(); off.assign(1, 0); }
+    void push(const uint32_t *p, size_t n) {
+        data.insert(data.end(), p, p + n);
+        off.push_back(data.size());
+    }
+    // count rows of `each` words, back to back at p
+    void assign_fixed(const uint32_t *p, size_t count, size_t each) {
+        data.assign(p, p + count * each);
+        off.resize(count + 1);
+        for (size_t i = 0; i <= count; ++i) off[i] = i * each;
+    }
+};
 struct Opening {
-    std::vector<std::vector<uint32_t>> rows;  // opened_rows
-    ByteList merkle;                          // merkle_proof
+    WordList rows;    // opened_rows
+    ByteList merkle;  // merkle_proof
 };
 struct Proof {  // FinalizedLigeritoProof, src/data_structures.rs:91-103
     std::vector<uint8_t> initial_root;
