@@ -57,6 +57,20 @@ def test_host_input_column_groups_match_oracle(lg, ref, ctx, k):
     assert a == b == ref.prove(rc, poly, nthreads=8)
 
 
+def test_large_last_commitment_matches_oracle(lg, ref, ctx):
+    # The last opening normally reads host copies of the last commitment,
+    # fetched during the last rounds; this one (2^16 rows x 16 columns, 8 MB
+    # with its tree) is over that limit and is gathered on the device.
+    import os
+
+    pc = lg.ProverConfig(1, (1 << 18, 1 << 2), [(1 << 14, 1 << 4)], 2, [4])
+    rc = ref.config(1, 18, 2, [14], [4])
+    poly = lg.splitmix_coeffs(7, pc.poly_len)
+    got = lg.prover(pc, lg.to_device(poly), ctx).to_bytes()
+    assert got == ref.prove(rc, poly, nthreads=os.cpu_count() or 8)
+    assert lg.verifier(pc, got, ctx)
+
+
 def test_pinned_and_pageable_host_inputs_give_the_same_proof(lg, ctx):
     # the host paths overlap the input copy with the first commitment
     import torch
