@@ -855,22 +855,37 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
 
 template <class F>
 lg_status guarded(lg_ctx *c, F &&f) {
+    // A call that stops early may leave copies in flight into the context's
+    // pinned and device arenas; the next call reuses those from the start,
+    // so wait for both streams first (errors already reported are ignored).
+    auto drain = [c]() {
+        if (!c) return;
+        cudaStreamSynchronize(c->stream);
+        if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+        cudaGetLastError();
+    };
     try {
         f();
         return LG_OK;
     } catch (const CudaFail &) {
+        drain();
         return LG_ERR_CUDA;
     } catch (const OutOfBudget &) {
+        drain();
         return LG_ERR_OUT_OF_MEMORY;
     } catch (const ProverAssert &) {
+        drain();
         if (c) c->err = "prover assertion failed";
         return LG_ERR_PROVER_ASSERT;
     } catch (const VerifyPanic &) {
+        drain();
         if (c) c->err = "verifier panic";
         return LG_ERR_VERIFY_PANIC;
     } catch (const BadConfig &) {
+        drain();
         return LG_ERR_INVALID_CONFIG;
     } catch (const std::bad_alloc &) {
+        drain();
         if (c) c->err = "host allocation failed";
         return LG_ERR_OUT_OF_MEMORY;
     }
