@@ -207,6 +207,29 @@ std::array<uint64_t, 2> Transcript::squeeze() {
     for (int i = 15; i >= 8; --i) hi = (hi << 8) | d[i];
     return {lo, hi};
 }
+// The low 64 bits of squeeze(): the counter's 4 bytes join the pending
+// bytes (a block is compressed when they fill one), then a copy of the
+// state is finalised straight from the pending bytes; the result is the
+// first 8 digest bytes read little-endian.
+uint64_t Transcript::squeeze_lo() {
+    const uint8_t c4[4] = {(uint8_t)counter, (uint8_t)(counter >> 8), (uint8_t)(counter >> 16),
+                           (uint8_t)(counter >> 24)};
+    counter += 1;
+    h.update(c4, 4);
+    uint32_t st[8];
+    std::memcpy(st, h.h, sizeof st);
+    alignas(16) uint8_t tail[128];
+    const size_t n = h.n, tl = (n + 1 + 8 <= 64) ? 64 : 128;
+    std::memcpy(tail, h.buf, n);
+    tail[n] = 0x80;
+    std::memset(tail + n + 1, 0, tl - 8 - (n + 1));
+    const uint64_t bits = h.total * 8;
+    for (int i = 0; i < 8; ++i) tail[tl - 1 - i] = (uint8_t)(bits >> (8 * i));
+    sha256_block(st, tail);
+    if (tl == 128) sha256_block(st, tail + 64);
+    return (uint64_t)__builtin_bswap32(st[0]) | ((uint64_t)__builtin_bswap32(st[1]) << 32);
+}
+
 // get_distinct_queries (src/emulated_fs.rs:61-76)
 bool Transcript::get_distinct_queries(uint64_t n, size_t s, std::vector<uint64_t> &out) {
     out.clear();

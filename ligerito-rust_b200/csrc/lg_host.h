@@ -43,7 +43,8 @@ struct Transcript {
     void absorb_u32s(const uint32_t *v, size_t n);  // to_bytes of each, LE
     std::array<uint64_t, 2> squeeze();               // low, high 64 bits of the u128
     uint32_t get_field() { return (uint32_t)squeeze()[0]; }
-    uint64_t get_query(uint64_t n) { return squeeze()[0] % n; }
+    uint64_t get_query(uint64_t n) { return squeeze_lo() % n; }
+    uint64_t squeeze_lo();  // squeeze()[0] without the high half or the byte round trip
     // rejection of repeats, then sorted; false where the reference loops forever
     bool get_distinct_queries(uint64_t n, size_t s, std::vector<uint64_t> &out);
 };
