@@ -397,8 +397,8 @@ std::pair<const uint32_t *, const uint64_t *> open_rows(lg_ctx *c, Scratch &sc, 
     for (size_t i = 0; i < nr; ++i) idx[nq + i] = layer_off[refs[i].layer] + refs[i].index;
     const uint64_t *d_idx = sc.upload(idx.data(), idx.size());
     uint32_t *d_out = static_cast<uint32_t *>(sc.dev((nq * w.cols + nr * 8) * 4 + 16));
-    CK(c, lgk::gather_rows(c->L, w.E.u32(), w.rows, w.cols, d_idx, (uint32_t)nq, d_out));
-    CK(c, lgk::gather_nodes(c->L, w.tree.u32(), d_idx + nq, (uint32_t)nr, d_out + nq * w.cols));
+    CK(c, lgk::gather_opening(c->L, w.E.u32(), w.rows, w.cols, d_idx, (uint32_t)nq, w.tree.u32(), d_idx + nq,
+                              (uint32_t)nr, nullptr, d_out));
     const uint32_t *h = sc.download_later(d_out, nq * w.cols + nr * 8);
     const uint32_t cols = w.cols;
     sc.finalizers.push_back([h, nq, nr, cols, out]() {
@@ -438,8 +438,7 @@ std::pair<const uint32_t *, const uint64_t *> open_rows_dev(lg_ctx *c, Scratch &
     a.out = out;
     a.mirror = absorb_mirror;
     CK(c, lgk::fs_queries(c->L, fs, a));
-    CK(c, lgk::gather_rows(c->L, w.E.u32(), w.rows, w.cols, d_q, nq, d_out));
-    CK(c, lgk::gather_nodes(c->L, w.tree.u32(), d_nodes, cap, d_out + nq * w.cols, d_cnt));
+    CK(c, lgk::gather_opening(c->L, w.E.u32(), w.rows, w.cols, d_q, nq, w.tree.u32(), d_nodes, cap, d_cnt, d_out));
     const uint32_t *h = sc.download_deferred(d_out, nq * w.cols + (size_t)cap * 8 + 1);
     const uint32_t cols = w.cols;
     sc.finalizers.push_back([h, nq, cap, cols, op]() {

@@ -788,33 +788,33 @@ cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
 }
 
 // ============================================================== gathers
-__global__ void k_gather_rows(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
-                              const uint64_t *__restrict__ q, uint32_t nq, uint32_t *__restrict__ out) {
+// An opening in one launch: threads below nq*ncols copy the opened rows
+// (row q[k] of every column), the rest the 8 words of each Merkle node
+// (the node count on the device when d_count is given, at most count).
+__global__ void k_gather_opening(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
+                                 const uint64_t *__restrict__ q, uint32_t nq, const uint32_t *__restrict__ tree,
+                                 const uint64_t *__restrict__ node_idx, uint32_t count, const uint32_t *d_count,
+                                 uint32_t *__restrict__ out) {
     pdl_begin();
-    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= nq * ncols) return;
-    const uint32_t k = idx / ncols, j = idx % ncols;
-    out[idx] = E[(uint64_t)j * rows + q[k]];
-}
-cudaError_t gather_rows(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols,
-                        const uint64_t *d_queries, uint32_t nq, uint32_t *out) {
-    const uint32_t total = nq * ncols;
-    LGK_LAUNCH(L, "gather_rows", launch_k(k_gather_rows, (total + 255) / 256, 256, 0, L.stream, E, rows, ncols, d_queries, nq, out));
-    return cudaGetLastError();
-}
-__global__ void k_gather_nodes(const uint32_t *__restrict__ tree, const uint64_t *__restrict__ idx,
-                               uint32_t count, const uint32_t *d_count, uint32_t *__restrict__ out) {
-    pdl_begin();
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, nrow = nq * ncols;
+    if (t < nrow) {
+        const uint32_t k = t / ncols, j = t % ncols;
+        out[t] = E[(uint64_t)j * rows + q[k]];
+        return;
+    }
+    const uint32_t u = t - nrow;
     if (d_count) count = min(count, *d_count);
-    if (t >= count * 8) return;
-    out[t] = tree[8 * idx[t / 8] + (t % 8)];
+    if (u >= count * 8) return;
+    out[t] = tree[8 * node_idx[u / 8] + (u % 8)];
 }
-cudaError_t gather_nodes(Launcher &L, const uint32_t *tree, const uint64_t *d_node_index, uint32_t count,
-                         uint32_t *out, const uint32_t *d_count) {
-    if (count == 0) return cudaSuccess;
-    LGK_LAUNCH(L, "gather_nodes",
-               launch_k(k_gather_nodes, (count * 8 + 255) / 256, 256, 0, L.stream, tree, d_node_index, count, d_count, out));
+cudaError_t gather_opening(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, const uint64_t *d_queries,
+                           uint32_t nq, const uint32_t *tree, const uint64_t *d_node_index, uint32_t count,
+                           const uint32_t *d_count, uint32_t *out) {
+    const uint64_t total = (uint64_t)nq * ncols + 8ull * count;
+    if (total == 0) return cudaSuccess;
+    if (total > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    LGK_LAUNCH(L, "gather_opening", launch_k(k_gather_opening, (unsigned)((total + 255) / 256), 256, 0, L.stream, E,
+                                             rows, ncols, d_queries, nq, tree, d_node_index, count, d_count, out));
     return cudaGetLastError();
 }
 

@@ -126,11 +126,11 @@ cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint3
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves);
 
 // --- gathers for openings (src/ligero.rs:40-51, src/merkle_tree.rs:98) ---
-cudaError_t gather_rows(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols,
-                        const uint64_t *d_queries, uint32_t nq, uint32_t *out);
-// count nodes, or min(count, *d_count) when d_count is given
-cudaError_t gather_nodes(Launcher &L, const uint32_t *tree, const uint64_t *d_node_index,
-                         uint32_t count, uint32_t *out, const uint32_t *d_count = nullptr);
+// out = the nq opened rows (nq x ncols words), then count Merkle nodes (8
+// words each; min(count, *d_count) of them when d_count is given)
+cudaError_t gather_opening(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, const uint64_t *d_queries,
+                           uint32_t nq, const uint32_t *tree, const uint64_t *d_node_index, uint32_t count,
+                           const uint32_t *d_count, uint32_t *out);
 
 // --- multilinear folds (src/multilinear_poly.rs:66-87) -------------------
 // out[i] = sum_j gr[j] * in[j*M + i], M = 2^log_len >> k, 1 <= k <= 6;
