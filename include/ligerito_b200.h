@@ -231,6 +231,15 @@ lg_status lg_induce_sumcheck_poly_noalloc(void *stream, uint32_t n, const uint32
                                           const uint64_t *d_queries, uint32_t alpha, uint32_t *d_basis_out,
                                           uint32_t *d_enforced_sum);
 
+/* BinaryElem128 multiplication (define_galois_field!(BinaryElem128, u128,
+ * 0x87, ...), src/binary_field.rs:182-189, with the generic product of
+ * :52-105): d_out[i] = d_a[i] * d_b[i] mod x^128 + x^7 + x^2 + x + 1 for n
+ * elements, each two little-endian u64 limbs (bits 0-63, then 64-127) in
+ * device memory; the arrays must be 16-byte aligned.  The reference prover
+ * uses only BinaryElem32; this is the 128-bit field for a 128-bit-challenge
+ * variant. */
+lg_status lg_gf128_mul(lg_ctx *ctx, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t n);
+
 /* Seeded coefficient generator (SplitMix64; coefficient i = low 32 bits of
  * output i).  The reference draws unseeded rand::random (src/main.rs:25). */
 lg_status lg_fill_splitmix(lg_ctx *ctx, uint64_t seed, uint32_t *d_out, uint64_t n);

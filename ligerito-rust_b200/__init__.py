@@ -108,6 +108,7 @@ def _load() -> ctypes.CDLL:
         "lg_proof_size": (i32, [P, P]),
         "lg_compute_twiddles": (i32, [u32, P]),
         "lg_fft": (i32, [P, P, u32, u64]),
+        "lg_gf128_mul": (i32, [P, P, P, P, u64]),
         "lg_ifft": (i32, [P, P, u32, u64]),
         "lg_rs_encode_cols": (i32, [P, P, u32, u32, P]),
         "lg_ligero_commit": (i32, [P, P, u32, u32, P, P, P]),
@@ -623,6 +624,23 @@ def splitmix_coeffs(seed: int, n: int) -> np.ndarray:
     """Seeded coefficients: SplitMix64, coefficient i = low 32 bits of output i."""
     out = np.empty(n, dtype=np.uint32)
     lib.lg_fill_splitmix_host(seed, out.ctypes.data, n)
+    return out
+
+
+def gf128_mul(a, b, ctx: Optional[Context] = None):
+    """BinaryElem128 products a[i] * b[i] (src/binary_field.rs:182-189) of
+    two CUDA int64 tensors of shape (n, 2): each row is an element's low and
+    high 64 bits.  Returns a new tensor of the same shape."""
+    import torch
+
+    ctx = ctx or default_context()
+    if a.shape != b.shape or a.dim() != 2 or a.shape[1] != 2 or a.dtype != torch.int64 or b.dtype != torch.int64:
+        raise ValueError("gf128_mul wants two int64 tensors of shape (n, 2)")
+    if not (a.is_cuda and b.is_cuda):
+        raise LigeritoError(1, "expected CUDA tensors")
+    a, b = a.contiguous(), b.contiguous()
+    out = torch.empty_like(a)
+    _check(lib.lg_gf128_mul(ctx.handle, a.data_ptr(), b.data_ptr(), out.data_ptr(), a.shape[0]), ctx)
     return out
 
 

@@ -1269,6 +1269,16 @@ lg_status lg_fill_splitmix(lg_ctx *c, uint64_t seed, uint32_t *d_out, uint64_t n
     });
 }
 
+lg_status lg_gf128_mul(lg_ctx *c, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, uint64_t n) {
+    if (!c || (n && (!d_a || !d_b || !d_out))) return LG_ERR_INVALID_ARGUMENT;
+    if ((uintptr_t)d_a % 16 || (uintptr_t)d_b % 16 || (uintptr_t)d_out % 16) return LG_ERR_INVALID_ARGUMENT;
+    return guarded(c, [&] {
+        CK(c, cudaSetDevice(c->device));
+        CK(c, lgk::gf128_mul(c->L, d_a, d_b, d_out, n));
+        sync(c);
+    });
+}
+
 void lg_fill_splitmix_host(uint64_t seed, uint32_t *out, uint64_t n) {
     if (out) lg::splitmix_fill(seed, out, n, 0);
 }

@@ -49,7 +49,10 @@ __device__ __forceinline__ uint32_t gf_reduce(uint32_t hi, uint32_t lo) {
     return lo ^ lo2 ^ red_small(ov);
 }
 
-__device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
+// Carry-less 32 x 32 -> 64-bit product: 16 integer multiplies of operands
+// masked to every 4th bit (at most 8 ones meet at a position, so sums never
+// carry into the next position of the same class).
+__device__ __forceinline__ uint64_t clmul32(uint32_t a, uint32_t b) {
     const uint32_t m0 = 0x11111111u, m1 = 0x22222222u, m2 = 0x44444444u, m3 = 0x88888888u;
     uint32_t a0 = a & m0, a1 = a & m1, a2 = a & m2, a3 = a & m3;
     uint32_t b0 = b & m0, b1 = b & m1, b2 = b & m2, b3 = b & m3;
@@ -57,9 +60,36 @@ __device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
     uint64_t z1 = ((uint64_t)a0 * b1) ^ ((uint64_t)a1 * b0) ^ ((uint64_t)a2 * b3) ^ ((uint64_t)a3 * b2);
     uint64_t z2 = ((uint64_t)a0 * b2) ^ ((uint64_t)a1 * b1) ^ ((uint64_t)a2 * b0) ^ ((uint64_t)a3 * b3);
     uint64_t z3 = ((uint64_t)a0 * b3) ^ ((uint64_t)a1 * b2) ^ ((uint64_t)a2 * b1) ^ ((uint64_t)a3 * b0);
-    uint64_t r = (z0 & 0x1111111111111111ull) | (z1 & 0x2222222222222222ull) |
-                 (z2 & 0x4444444444444444ull) | (z3 & 0x8888888888888888ull);
+    return (z0 & 0x1111111111111111ull) | (z1 & 0x2222222222222222ull) | (z2 & 0x4444444444444444ull) |
+           (z3 & 0x8888888888888888ull);
+}
+
+__device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t b) {
+    const uint64_t r = clmul32(a, b);
     return gf_reduce((uint32_t)(r >> 32), (uint32_t)r);
+}
+
+// ------------------------------------------------------------ GF(2^128)
+// BinaryElem128 (x^128 + x^7 + x^2 + x + 1): two u64 limbs, low first.
+struct U128 {
+    uint64_t lo, hi;
+};
+// carry-less 64 x 64 -> 128 by Karatsuba over 32-bit halves (3 clmul32)
+__device__ __forceinline__ U128 clmul64(uint64_t a, uint64_t b) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    const uint64_t lo = clmul32(a0, b0), hi = clmul32(a1, b1), mid = clmul32(a0 ^ a1, b0 ^ b1) ^ lo ^ hi;
+    return {lo ^ (mid << 32), hi ^ (mid >> 32)};
+}
+// product by Karatsuba over 64-bit halves (9 clmul32), then the 256-bit
+// product's top half H folds down as H * (x^7 + x^2 + x + 1); the at most
+// 7 bits that H * x^k (k = 1, 2, 7) pushes past x^127 fold once more.
+__device__ __forceinline__ U128 gf128_mul(U128 a, U128 b) {
+    const U128 l = clmul64(a.lo, b.lo), h = clmul64(a.hi, b.hi), m = clmul64(a.lo ^ a.hi, b.lo ^ b.hi);
+    const uint64_t p0 = l.lo, p1 = l.hi ^ m.lo ^ l.lo ^ h.lo, p2 = h.lo ^ m.hi ^ l.hi ^ h.hi, p3 = h.hi;
+    const uint64_t ov = (p3 >> 63) ^ (p3 >> 62) ^ (p3 >> 57);
+    const uint64_t r0 = p0 ^ p2 ^ (p2 << 1) ^ (p2 << 2) ^ (p2 << 7) ^ ov ^ (ov << 1) ^ (ov << 2) ^ (ov << 7);
+    const uint64_t r1 = p1 ^ p3 ^ (p3 << 1) ^ (p2 >> 63) ^ (p3 << 2) ^ (p2 >> 62) ^ (p3 << 7) ^ (p2 >> 57);
+    return {r0, r1};
 }
 
 // ---------------------------------------------------------------- MulTab

@@ -1168,6 +1168,27 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
     return cudaGetLastError();
 }
 
+// ============================================================ GF(2^128)
+// out[i] = a[i] * b[i] in BinaryElem128, elements as two u64 limbs (low
+// first), 16-byte loads and stores.
+__global__ void k_gf128_mul(const ulonglong2 *__restrict__ a, const ulonglong2 *__restrict__ b,
+                            ulonglong2 *__restrict__ out, uint64_t n) {
+    pdl_begin();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const ulonglong2 x = a[i], y = b[i];
+        const U128 r = lgd::gf128_mul({x.x, x.y}, {y.x, y.y});
+        out[i] = make_ulonglong2(r.lo, r.hi);
+    }
+}
+cudaError_t gf128_mul(Launcher &L, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t n) {
+    if (n == 0) return cudaSuccess;
+    if ((uintptr_t)a % 16 || (uintptr_t)b % 16 || (uintptr_t)out % 16) return cudaErrorInvalidValue;
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 8);
+    LGK_LAUNCH(L, "gf128_mul", launch_k(k_gf128_mul, blocks, 256, 0, L.stream, reinterpret_cast<const ulonglong2 *>(a),
+                                        reinterpret_cast<const ulonglong2 *>(b), reinterpret_cast<ulonglong2 *>(out), n));
+    return cudaGetLastError();
+}
+
 // ============================================================== splitmix
 __global__ void k_splitmix(uint64_t seed, uint32_t *out, uint64_t n) {
     pdl_begin();

@@ -178,6 +178,11 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
 
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);
 
+// --- BinaryElem128 (src/binary_field.rs:182-189) --------------------------
+// out[i] = a[i] * b[i], n elements of two u64 limbs (low first), 16-byte
+// aligned device arrays.
+cudaError_t gf128_mul(Launcher &L, const uint64_t *a, const uint64_t *b, uint64_t *out, uint64_t n);
+
 // --- Fiat-Shamir transcript on the device (src/emulated_fs.rs:6-76) ------
 // The running SHA-256 of the transcript: the host's lg::Transcript with the
 // pending bytes kept as big-endian words (the transcript only ever absorbs

@@ -155,3 +155,34 @@ def test_bad_arguments_return_status(lg, ctx):
         lg.fft(lg.to_device(np.zeros(8, np.uint32)), 0, ctx)
     assert lg.lib.lg_fft(ctx.handle, None, 4, 1) == 1
     assert lg.lib.lg_partial_eval(ctx.handle, None, 4, None, 1, None) == 1
+
+
+def test_gf128_mul_matches_oracle(lg, ref, ctx):
+    # BinaryElem128 (src/binary_field.rs:182-189): device products against
+    # the oracle's on random pairs, edge values and a ragged count
+    import ctypes
+
+    import torch
+
+    n = 4099
+    r = np.random.default_rng(128)
+    a = r.integers(0, np.iinfo(np.uint64).max, size=(n, 2), dtype=np.uint64, endpoint=True)
+    b = r.integers(0, np.iinfo(np.uint64).max, size=(n, 2), dtype=np.uint64, endpoint=True)
+    top = np.iinfo(np.uint64).max
+    edges = [(0, 0), (1, 0), (top, top), (0, 1 << 63), (1 << 63, 0), (0, 1), (0x87, 0), (2, 0)]
+    for i, e in enumerate(edges):
+        for j, f in enumerate(edges):
+            a[i * len(edges) + j] = e
+            b[i * len(edges) + j] = f
+    dev = lambda x: torch.from_numpy(x.view(np.int64)).cuda()  # noqa: E731
+    got = lg.gf128_mul(dev(a), dev(b), ctx).cpu().numpy().view(np.uint64)
+    A, B, O = (ctypes.c_uint64 * 2)(), (ctypes.c_uint64 * 2)(), (ctypes.c_uint64 * 2)()
+    for i in range(n):
+        A[0], A[1], B[0], B[1] = int(a[i, 0]), int(a[i, 1]), int(b[i, 0]), int(b[i, 1])
+        ref.lib().lgref_gf128_mul(A, B, O)
+        assert (int(got[i, 0]), int(got[i, 1])) == (O[0], O[1]), i
+    # no elements; misaligned arrays are refused
+    z = torch.zeros((0, 2), dtype=torch.int64, device="cuda")
+    assert lg.gf128_mul(z, z, ctx).shape == (0, 2)
+    t = torch.zeros(9, dtype=torch.int64, device="cuda")
+    assert lg.lib.lg_gf128_mul(ctx.handle, t.data_ptr() + 8, t.data_ptr(), t.data_ptr(), 1) == 1
