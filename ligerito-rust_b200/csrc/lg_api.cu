@@ -743,6 +743,37 @@ void ligero_verify_host(const std::vector<uint64_t> &q, const lg::Opening &o, co
     }
 }
 
+// The same check with the per-row work on the device: every panic that
+// does not depend on the field values is decided on the host first, then
+// one block per opened row compares <row, gr> with <yr, basis>.
+void ligero_verify_dev(lg_ctx *c, Scratch &sc, const std::vector<uint64_t> &q, const lg::Opening &o,
+                       const std::vector<uint32_t> &yr, const std::vector<uint32_t> &ch) {
+    const size_t ylen = yr.size();
+    if (ylen == 0 || (ylen & (ylen - 1))) throw VerifyPanic{};
+    uint32_t nv = 0;
+    while ((1ull << nv) < ylen) ++nv;
+    if (nv > 31) return ligero_verify_host(q, o, yr, ch);
+    const size_t nrows = o.rows.size();
+    if (nrows > q.size()) throw VerifyPanic{};
+    for (size_t i = 0; i < nrows; ++i)
+        if (q[i] > 0xFFFFFFFFull) throw VerifyPanic{};
+    if (nrows == 0) return;
+    const std::vector<uint32_t> gr = lg::lagrange_basis(ch.data(), ch.size());
+    const std::vector<uint32_t> sks = lg::eval_sk_at_vks(ylen);
+    const uint32_t *d_rows = sc.upload(o.rows.data.data(), o.rows.data.size());
+    const uint64_t *d_off = sc.upload(o.rows.off.data(), o.rows.off.size());
+    const uint32_t *d_gr = sc.upload(gr.data(), gr.size());
+    const uint32_t *d_yr = sc.upload(yr.data(), ylen);
+    const uint64_t *d_q = sc.upload(q.data(), nrows);
+    uint32_t *d_bad = static_cast<uint32_t *>(sc.dev(4));
+    CK(c, cudaMemsetAsync(d_bad, 0, 4, c->stream));
+    CK(c, lgk::ligero_check(c->L, d_rows, d_off, (uint32_t)nrows, d_gr, (uint32_t)gr.size(), d_yr, nv, d_q,
+                            sks.data(), d_bad));
+    uint32_t bad = 0;
+    d2h(c, &bad, d_bad, 4);
+    if (bad) throw VerifyPanic{};
+}
+
 bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &P) {
     const size_t s = LG_NUM_QUERIES;
     const uint32_t log_inv_rate = 2;  // src/verifier.rs:26
@@ -795,7 +826,7 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
             depth = cfg.log_m[i] + log_inv_rate;
             if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};
             if (!opening_ok(root, P.final_, depth, q)) throw VerifyPanic{};
-            ligero_verify_host(q, P.final_, P.yr, rs);
+            ligero_verify_dev(c, sc, q, P.final_, P.yr, rs);
             const uint32_t final_r = fs.get_field();  // :114
             const size_t yl = P.yr.size();
             if (yl < 2) throw VerifyPanic{};

@@ -1168,6 +1168,65 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
     return cudaGetLastError();
 }
 
+// ======================================================= ligero_verify
+// One block per opened row k: dot = <row_k, gr> over the first min(row
+// length, glen) entries (zip truncation), e = sum_j yr[j] * basis_k[j]
+// with basis_k[j] the product of sx[t] over the set bits t of j, sx[0] =
+// q_k and sx[t] = sx[t-1]^2 + sks[t-1] sx[t-1]; a mismatch sets *bad.
+// The product form gives the same field elements as the reference's
+// doubling (src/ligero.rs:97-131, evaluate_scaled_basis_inplace).
+__global__ void __launch_bounds__(256) k_ligero_check(const uint32_t *__restrict__ rows,
+                                                      const uint64_t *__restrict__ row_off, uint32_t nrows,
+                                                      const uint32_t *__restrict__ gr, uint32_t glen,
+                                                      const uint32_t *__restrict__ yr, uint32_t nv,
+                                                      const uint64_t *__restrict__ q, ligero_sks sks,
+                                                      uint32_t *bad) {
+    pdl_begin();
+    __shared__ uint32_t sx[32];
+    __shared__ uint32_t part[2][8];
+    const uint32_t k = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (k >= nrows) return;
+    if (threadIdx.x == 0) {
+        uint32_t s = (uint32_t)q[k];
+        sx[0] = s;
+        for (uint32_t t = 1; t < nv; ++t) {
+            s = gf_mul(s, s) ^ gf_mul(sks.v[t - 1], s);
+            sx[t] = s;
+        }
+    }
+    __syncthreads();
+    const uint64_t r0 = row_off[k], rlen = row_off[k + 1] - r0, zl = rlen < glen ? rlen : (uint64_t)glen;
+    uint32_t dot = 0, e = 0;
+    for (uint64_t j = threadIdx.x; j < zl; j += blockDim.x) dot ^= gf_mul(rows[r0 + j], gr[j]);
+    const uint32_t ylen = 1u << nv;
+    for (uint32_t j = threadIdx.x; j < ylen; j += blockDim.x) {
+        uint32_t b = 1;
+        for (uint32_t t = 0; t < nv; ++t)
+            if ((j >> t) & 1) b = gf_mul(b, sx[t]);
+        e ^= gf_mul(yr[j], b);
+    }
+    dot = warp_xor(dot);
+    e = warp_xor(e);
+    if (lane == 0) { part[0][warp] = dot; part[1][warp] = e; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t d = 0, s = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) { d ^= part[0][w]; s ^= part[1][w]; }
+        if (d != s) atomicOr(bad, 1u);
+    }
+}
+cudaError_t ligero_check(Launcher &L, const uint32_t *rows, const uint64_t *row_off, uint32_t nrows,
+                         const uint32_t *gr, uint32_t glen, const uint32_t *yr, uint32_t nv, const uint64_t *q,
+                         const uint32_t *sks, uint32_t *bad) {
+    if (nrows == 0) return cudaSuccess;
+    if (nv > 31) return cudaErrorInvalidValue;
+    ligero_sks s{};
+    for (uint32_t t = 0; t + 1 < nv; ++t) s.v[t] = sks[t];
+    LGK_LAUNCH(L, "ligero_check", launch_k(k_ligero_check, nrows, 256, 0, L.stream, rows, row_off, nrows, gr, glen,
+                                           yr, nv, q, s, bad));
+    return cudaGetLastError();
+}
+
 // ============================================================ GF(2^128)
 // out[i] = a[i] * b[i] in BinaryElem128, elements as two u64 limbs (low
 // first), 16-byte loads and stores.

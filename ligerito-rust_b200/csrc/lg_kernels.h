@@ -178,6 +178,16 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
 
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);
 
+// --- ligero_verify (src/ligero.rs:97-131) ----------------------------------
+// Rows k < nrows at rows[row_off[k] .. row_off[k+1]), the Lagrange basis gr
+// of the challenges (glen words), yr (2^nv words), the queries q and
+// eval_sk_at_vks's first nv - 1 values; *bad (zeroed by the caller) becomes
+// nonzero if any row's check fails.
+struct ligero_sks { uint32_t v[32]; };
+cudaError_t ligero_check(Launcher &L, const uint32_t *rows, const uint64_t *row_off, uint32_t nrows,
+                         const uint32_t *gr, uint32_t glen, const uint32_t *yr, uint32_t nv, const uint64_t *q,
+                         const uint32_t *sks, uint32_t *bad);
+
 // --- BinaryElem128 (src/binary_field.rs:182-189) --------------------------
 // out[i] = a[i] * b[i], n elements of two u64 limbs (low first), 16-byte
 // aligned device arrays.
