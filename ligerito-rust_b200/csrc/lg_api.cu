@@ -686,8 +686,8 @@ Quad quad_from_evals(uint32_t at0, uint32_t at1, uint32_t atx) {  // :67-81, x =
 uint32_t eval_quad(const Quad &p, uint32_t r) { return lg::gf_mul(lg::gf_mul(p.a, r), r) ^ lg::gf_mul(p.b, r) ^ p.c; }
 
 // merkle_tree::verify of an opening (leaf bytes = LE words of each row)
-bool opening_ok(const std::vector<uint8_t> &root, const lg::Opening &o, size_t depth,
-                const std::vector<uint64_t> &q) {
+bool opening_ok_host(const std::vector<uint8_t> &root, const lg::Opening &o, size_t depth,
+                     const std::vector<uint64_t> &q) {
     if (o.rows.size() < q.size()) return false;  // layer index panic
     std::vector<std::array<uint8_t, 32>> layer(q.size());
     std::vector<uint8_t> buf;
@@ -703,6 +703,38 @@ bool opening_ok(const std::vector<uint8_t> &root, const lg::Opening &o, size_t d
     bool ok = false;
     if (!lg::merkle_verify(root.data(), root.size(), o.merkle, depth, layer, q, &ok)) return false;
     return ok;
+}
+
+// The same check on the device when the opening is well formed (the first
+// nq rows of one length, 1..256 words; sorted distinct queries inside the
+// tree; every proof node the opening consumes present and 32 bytes), which
+// are exactly the cases where the host walk neither panics nor meets a
+// sibling of another length.  Anything else takes the host walk.
+bool opening_ok(lg_ctx *c, Scratch &sc, const std::vector<uint8_t> &root, const lg::Opening &o, size_t depth,
+                const std::vector<uint64_t> &q) {
+    const size_t nq = q.size();
+    bool fast = nq >= 1 && nq <= 256 && o.rows.size() >= nq && depth >= 1 && depth <= 63;
+    const size_t ncols = fast ? o.rows.len(0) : 0;
+    for (size_t i = 0; fast && i < nq; ++i)
+        fast = o.rows.len(i) == ncols && (i == 0 || q[i] > q[i - 1]) && (q[i] >> depth) == 0;
+    fast = fast && ncols >= 1 && ncols <= 256;
+    std::vector<NodeRef> refs;
+    if (fast) {
+        lg::merkle_proof_nodes(q, 1ull << depth, refs);
+        fast = o.merkle.size() >= refs.size();
+        for (size_t j = 0; fast && j < refs.size(); ++j) fast = o.merkle.len(j) == 32;
+    }
+    if (!fast) return opening_ok_host(root, o, depth, q);
+    const uint32_t *d_rows = sc.upload(o.rows.data.data(), nq * ncols);
+    const uint64_t *d_q = sc.upload(q.data(), nq);
+    const uint32_t *d_proof = refs.empty() ? nullptr
+                                           : sc.upload(reinterpret_cast<const uint32_t *>(o.merkle.data.data()),
+                                                       8 * refs.size());
+    uint32_t *d_out = static_cast<uint32_t *>(sc.dev(9 * 4));
+    CK(c, lgk::opening_check(c->L, d_rows, (uint32_t)ncols, d_q, (uint32_t)nq, d_proof, (uint32_t)depth, d_out));
+    uint32_t out[9];
+    d2h(c, out, d_out, sizeof out);
+    return out[8] == 1 && root.size() == 32 && std::memcmp(out, root.data(), 32) == 0;
 }
 
 std::vector<uint32_t> dense(const lg::Opening &o, size_t want_rows, size_t want_len) {
@@ -786,7 +818,7 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
     size_t depth = cfg.initial_log_m + log_inv_rate;
     std::vector<uint64_t> q;
     if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};
-    if (!opening_ok(P.initial_root, P.initial, depth, q)) throw VerifyPanic{};  // :42-49
+    if (!opening_ok(c, sc, P.initial_root, P.initial, depth, q)) throw VerifyPanic{};  // :42-49
     const uint32_t alpha = fs.get_field();
     std::vector<uint32_t> rows = dense(P.initial, s, 1ull << cfg.initial_k);
     std::vector<DBuf> basis;
@@ -825,7 +857,7 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
             fs.absorb_u32s(P.yr.data(), P.yr.size());
             depth = cfg.log_m[i] + log_inv_rate;
             if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};
-            if (!opening_ok(root, P.final_, depth, q)) throw VerifyPanic{};
+            if (!opening_ok(c, sc, root, P.final_, depth, q)) throw VerifyPanic{};
             ligero_verify_dev(c, sc, q, P.final_, P.yr, rs);
             const uint32_t final_r = fs.get_field();  // :114
             const size_t yl = P.yr.size();
@@ -863,7 +895,7 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
         fs.absorb(P.recursive_roots[i + 1].data(), P.recursive_roots[i + 1].size());  // :122
         depth = cfg.log_m[i] + log_inv_rate;
         if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};  // :126
-        if (!opening_ok(root, P.recursive[i], depth, q)) throw VerifyPanic{};
+        if (!opening_ok(c, sc, root, P.recursive[i], depth, q)) throw VerifyPanic{};
         const uint32_t al = fs.get_field();  // :345
         std::vector<uint32_t> rr = dense(P.recursive[i], s, 1ull << cfg.ks[i]);
         basis.emplace_back(c, 4ull << cfg.log_m[i]);

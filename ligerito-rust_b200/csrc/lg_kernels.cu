@@ -1168,6 +1168,101 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
     return cudaGetLastError();
 }
 
+// ====================================================== opening check
+// merkle_tree::verify of one opening (src/merkle_tree.rs:120-188) for
+// well-formed inputs, in one block: nq <= 256 sorted distinct queries, their
+// rows of ncols words (1..256) hashed as the leaves, and at least as many
+// 32-byte proof nodes as the opening consumes.  Each layer up, entry i
+// starts a step unless it is the right partner of i-1 (q[i-1] even and
+// q[i] = q[i-1] + 1); a step pairs with its right partner or takes the next
+// proof node (on the left when q[i] is odd); the steps in order are the next
+// layer.  out = the last layer's first hash (8 words) and its size.
+__global__ void __launch_bounds__(256) k_opening_check(const uint32_t *__restrict__ rows, uint32_t ncols,
+                                                       const uint64_t *__restrict__ q, uint32_t nq,
+                                                       const uint32_t *__restrict__ proof, uint32_t depth,
+                                                       uint32_t *__restrict__ out, uint32_t one) {
+    pdl_begin();
+    __shared__ uint32_t h[256][8];
+    __shared__ uint64_t qs[256];
+    __shared__ uint32_t cnt[2][8];
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarps = blockDim.x >> 5;
+    if (t < nq) {
+        const uint32_t nb = (ncols + 15) / 16;
+        uint32_t cv[8];
+        b3_iv(cv);
+        for (uint32_t b = 0; b < nb; ++b) {
+            uint32_t m[16];
+#pragma unroll
+            for (int w = 0; w < 16; ++w) {
+                const uint32_t j = b * 16 + w;
+                m[w] = j < ncols ? rows[(uint64_t)t * ncols + j] : 0u;
+            }
+            const bool last = b + 1 == nb;
+            const uint32_t blen = last ? 4 * ncols - 64 * (nb - 1) : 64;
+            const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
+            b3_compress(cv, m, blen, flags, one);
+        }
+#pragma unroll
+        for (int w = 0; w < 8; ++w) h[t][w] = cv[w];
+        qs[t] = q[t];
+    }
+    uint32_t cur = nq, pc_base = 0;
+    for (uint32_t d = 0; d < depth; ++d) {
+        __syncthreads();
+        const bool active = t < cur;
+        const uint64_t qi = active ? qs[t] : 0;
+        const bool right = active && t > 0 && !(qs[t - 1] & 1) && qi == qs[t - 1] + 1;
+        const bool start = active && !right;
+        const bool paired = start && t + 1 < cur && !(qi & 1) && qs[t + 1] == qi + 1;
+        const bool uses = start && !paired;
+        const uint32_t ms = __ballot_sync(0xffffffffu, start), mu = __ballot_sync(0xffffffffu, uses);
+        if (lane == 0) { cnt[0][warp] = __popc(ms); cnt[1][warp] = __popc(mu); }
+        __syncthreads();
+        uint32_t step = __popc(ms & ((1u << lane) - 1)), pidx = __popc(mu & ((1u << lane) - 1));
+        uint32_t nsteps = 0, nuses = 0;
+        for (uint32_t w = 0; w < nwarps; ++w) {
+            if (w < warp) { step += cnt[0][w]; pidx += cnt[1][w]; }
+            nsteps += cnt[0][w];
+            nuses += cnt[1][w];
+        }
+        uint32_t parent[8];
+        if (start) {
+            uint32_t mine[8], other[8];
+#pragma unroll
+            for (int w = 0; w < 8; ++w) mine[w] = h[t][w];
+            if (paired) {
+#pragma unroll
+                for (int w = 0; w < 8; ++w) other[w] = h[t + 1][w];
+                hash_node(mine, other, parent, one);
+            } else {
+                const uint32_t *nd = proof + 8ull * (pc_base + pidx);
+#pragma unroll
+                for (int w = 0; w < 8; ++w) other[w] = nd[w];
+                if (qi & 1) hash_node(other, mine, parent, one);
+                else hash_node(mine, other, parent, one);
+            }
+        }
+        __syncthreads();
+        if (start) {
+#pragma unroll
+            for (int w = 0; w < 8; ++w) h[step][w] = parent[w];
+            qs[step] = qi >> 1;
+        }
+        cur = nsteps;
+        pc_base += nuses;
+    }
+    __syncthreads();
+    if (t < 8) out[t] = h[0][t];
+    if (t == 8) out[8] = cur;
+}
+cudaError_t opening_check(Launcher &L, const uint32_t *rows, uint32_t ncols, const uint64_t *q, uint32_t nq,
+                          const uint32_t *proof, uint32_t depth, uint32_t *out) {
+    if (nq == 0 || nq > 256 || ncols == 0 || ncols > 256 || depth > 63) return cudaErrorInvalidValue;
+    LGK_LAUNCH(L, "opening_check", launch_k(k_opening_check, 1, 256, 0, L.stream, rows, ncols, q, nq, proof, depth,
+                                            out, 1u));
+    return cudaGetLastError();
+}
+
 // ======================================================= ligero_verify
 // One block per opened row k: dot = <row_k, gr> over the first min(row
 // length, glen) entries (zip truncation), e = sum_j yr[j] * basis_k[j]

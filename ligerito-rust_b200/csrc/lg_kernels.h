@@ -178,6 +178,14 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
 
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);
 
+// --- merkle_tree::verify of one opening (src/merkle_tree.rs:120-188) ------
+// Well-formed inputs only (the caller checks): nq <= 256 sorted distinct
+// queries, their rows (nq x ncols words, 1 <= ncols <= 256) and the 32-byte
+// proof nodes the opening consumes (8 words each, in order).  out (9 words)
+// = the last layer's first hash and the last layer's size.
+cudaError_t opening_check(Launcher &L, const uint32_t *rows, uint32_t ncols, const uint64_t *q, uint32_t nq,
+                          const uint32_t *proof, uint32_t depth, uint32_t *out);
+
 // --- ligero_verify (src/ligero.rs:97-131) ----------------------------------
 // Rows k < nrows at rows[row_off[k] .. row_off[k+1]), the Lagrange basis gr
 // of the challenges (glen words), yr (2^nv words), the queries q and
