@@ -342,6 +342,50 @@ def run_micro(args):
                       "kernel_ms": {k: [v[0], round(v[1], 4)] for k, v in stats.items()}}), flush=True)
 
 
+def run_verify(args):
+    """The verifier on one 2^24 proof (config_24, seed 1): lg_verify's wall
+    time per call from host proof bytes (its host transcript and the device
+    checks; synchronous), beside the oracle's verifier on all host cores
+    (a bounded sample of 3 calls)."""
+    import torch
+
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as g
+
+    lg = g.load_package()
+    ctx = lg.Context(0)
+    cfg = lg.hardcoded_config_24()
+    proof = lg.prover(cfg, lg.splitmix_coeffs_device(1, cfg.poly_len, ctx), ctx).to_bytes()
+    for _ in range(args.warmup):
+        assert lg.verifier(cfg, proof, ctx)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ok = lg.verifier(cfg, proof, ctx)
+        times.append((time.perf_counter() - t0) * 1e3)
+        assert ok
+    line = {"workload": "verify24", "metric": "verify ms of one 2^24 proof (config_24)",
+            "value": round(statistics.median(times), 4), "unit": "ms", "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "min_ms": round(min(times), 4), "proof_bytes": len(proof)}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import lgref
+
+        threads = os.cpu_count() or 1
+        rc = lgref.config_make(24)
+        cpu = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            st, ok = lgref.verify(rc, proof, nthreads=threads)
+            cpu.append((time.perf_counter() - t0) * 1e3)
+            assert st == lgref.OK and ok
+        line["cpu_baseline"] = {"value": round(statistics.median(cpu), 3), "unit": "ms", "cores": threads,
+                                "kind": "port", "sample": "3 verifications of the same proof by the C restatement "
+                                                          "under oracle/"}
+    print(json.dumps(line), flush=True)
+
+
 def _pct(xs, q):
     xs = sorted(xs)
     return xs[min(len(xs) - 1, int(round(q * (len(xs) - 1))))] if xs else None
@@ -498,7 +542,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="prove24",
                     choices=["prove24", "commit24", "fft16", "fft20", "fft22", "ifft16", "ifft20", "ifft22",
-                             "batch64", "serve"])
+                             "batch64", "serve", "verify24"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests per rate")
     ap.add_argument("--rates", default="500,1000,2000,4000,8000,16000", help="serve: offered rates (requests/s)")
@@ -510,6 +554,8 @@ def main():
         run_batch64(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "verify24":
+        run_verify(args)
     elif args.workload != "prove24":
         run_micro(args)
     else:
