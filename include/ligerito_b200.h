@@ -74,6 +74,15 @@ lg_status lg_config_make(uint32_t log_size, lg_config *out);
 /* The consistency the reference asserts while proving (src/prover.rs,
  * src/sumcheck_polys.rs:97): LG_OK or LG_ERR_INVALID_CONFIG. */
 lg_status lg_config_validate(const lg_config *cfg, uint64_t poly_len);
+/* A config as text, in place of the hard-coded ProverConfig values of
+ * src/config.rs:6-134: lines "key = values" for recursive_steps,
+ * initial_dims (rows columns), initial_k, dims (one "rows columns" pair per
+ * step, pairs separated by commas) and ks; '#' starts a comment; every
+ * dimension a power of two.  Parse errors are LG_ERR_INVALID_CONFIG; the
+ * result still goes through lg_config_validate when proving.  Format writes
+ * the same form with its terminating NUL (buf NULL: *len = the size). */
+lg_status lg_config_parse(const char *text, lg_config *out);
+lg_status lg_config_format(const lg_config *cfg, char *buf, uint64_t *len);
 
 /* ---------------------------------------------------------------- context */
 /* hbm_budget_bytes = 0: no budget.  Fails with LG_ERR_NO_DEVICE without a GPU. */

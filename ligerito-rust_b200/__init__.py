@@ -108,6 +108,8 @@ def _load() -> ctypes.CDLL:
         "lg_proof_size": (i32, [P, P]),
         "lg_compute_twiddles": (i32, [u32, P]),
         "lg_fft": (i32, [P, P, u32, u64]),
+        "lg_config_parse": (i32, [ctypes.c_char_p, P]),
+        "lg_config_format": (i32, [P, P, P]),
         "lg_gf128_mul": (i32, [P, P, P, P, u64]),
         "lg_ifft": (i32, [P, P, u32, u64]),
         "lg_rs_encode_cols": (i32, [P, P, u32, u32, P]),
@@ -243,6 +245,24 @@ def hardcoded_config_24() -> ProverConfig:
     c = LgConfig()
     _check(lib.lg_hardcoded_config_24(ctypes.byref(c)))
     return _from_c(c)
+
+
+def config_from_text(text: str) -> ProverConfig:
+    """A ProverConfig from its text form (lg_config_parse): lines
+    "key = values" for recursive_steps, initial_dims, initial_k, dims and ks."""
+    c = LgConfig()
+    _check(lib.lg_config_parse(text.encode(), ctypes.byref(c)))
+    return _from_c(c)
+
+
+def config_to_text(cfg: ProverConfig) -> str:
+    """The text form lg_config_parse reads back."""
+    c = cfg.to_c()
+    n = ctypes.c_uint64()
+    _check(lib.lg_config_format(ctypes.byref(c), None, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value)
+    _check(lib.lg_config_format(ctypes.byref(c), buf, ctypes.byref(n)))
+    return buf.value.decode()
 
 
 def hardcoded_config_20_verifier() -> VerifierConfig:

@@ -1024,6 +1024,117 @@ lg_status lg_config_validate(const lg_config *cfg, uint64_t poly_len) {
     return lg::config_check(*cfg, poly_len);
 }
 
+// Text form of a config (the fields of ProverConfig, src/config.rs:6-67),
+// one "key = values" per line, '#' to the end of a line is a comment:
+//   recursive_steps = 2
+//   initial_dims = 262144 64     (rows, columns of the first matrix)
+//   initial_k = 6
+//   dims = 16384 16, 1024 16     (one "rows columns" pair per step)
+//   ks = 4 4
+// Every dimension is a power of two.
+lg_status lg_config_parse(const char *text, lg_config *out) {
+    if (!text || !out) return LG_ERR_INVALID_ARGUMENT;
+    lg_config c{};
+    bool seen[5] = {false, false, false, false, false};
+    std::vector<uint64_t> dims;
+    std::vector<uint64_t> ks;
+    auto log2_exact = [](uint64_t v, uint32_t *lg) {
+        if (v == 0 || (v & (v - 1))) return false;
+        uint32_t l = 0;
+        while ((1ull << l) < v) ++l;
+        *lg = l;
+        return true;
+    };
+    std::string all(text);
+    size_t pos = 0;
+    while (pos <= all.size()) {
+        size_t eol = all.find('\n', pos);
+        if (eol == std::string::npos) eol = all.size();
+        std::string line = all.substr(pos, eol - pos);
+        pos = eol + 1;
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.resize(hash);
+        const size_t eq = line.find('=');
+        std::string key = line.substr(0, eq == std::string::npos ? line.size() : eq);
+        key.erase(0, key.find_first_not_of(" \t\r"));
+        key.erase(key.find_last_not_of(" \t\r") + 1);
+        if (key.empty() && eq == std::string::npos) continue;  // blank line
+        if (eq == std::string::npos) return LG_ERR_INVALID_CONFIG;
+        std::vector<uint64_t> vals;
+        std::string rest = line.substr(eq + 1);
+        for (char &ch : rest)
+            if (ch == ',') ch = ' ';
+        const char *p = rest.c_str();
+        while (*p) {
+            while (*p == ' ' || *p == '\t' || *p == '\r') ++p;
+            if (!*p) break;
+            if (*p < '0' || *p > '9') return LG_ERR_INVALID_CONFIG;
+            char *end = nullptr;
+            const unsigned long long v = std::strtoull(p, &end, 10);
+            if (end == p) return LG_ERR_INVALID_CONFIG;
+            vals.push_back(v);
+            p = end;
+        }
+        const char *keys[5] = {"recursive_steps", "initial_dims", "initial_k", "dims", "ks"};
+        int k = -1;
+        for (int i = 0; i < 5; ++i)
+            if (key == keys[i]) k = i;
+        if (k < 0 || seen[k]) return LG_ERR_INVALID_CONFIG;
+        seen[k] = true;
+        if (k == 0 || k == 2) {
+            if (vals.size() != 1 || vals[0] > 0xFFFFFFFFull) return LG_ERR_INVALID_CONFIG;
+            (k == 0 ? c.recursive_steps : c.initial_k) = (uint32_t)vals[0];
+        } else if (k == 1) {
+            if (vals.size() != 2 || !log2_exact(vals[0], &c.initial_log_m) || !log2_exact(vals[1], &c.initial_log_n))
+                return LG_ERR_INVALID_CONFIG;
+        } else if (k == 3) {
+            dims = vals;
+        } else {
+            ks = vals;
+        }
+    }
+    for (bool b : seen)
+        if (!b) return LG_ERR_INVALID_CONFIG;
+    if (c.recursive_steps < 1 || c.recursive_steps > LG_MAX_STEPS || dims.size() != 2ull * c.recursive_steps ||
+        ks.size() != c.recursive_steps)
+        return LG_ERR_INVALID_CONFIG;
+    for (uint32_t i = 0; i < c.recursive_steps; ++i) {
+        if (!log2_exact(dims[2 * i], &c.log_m[i]) || !log2_exact(dims[2 * i + 1], &c.log_n[i]) ||
+            ks[i] > 0xFFFFFFFFull)
+            return LG_ERR_INVALID_CONFIG;
+        c.ks[i] = (uint32_t)ks[i];
+    }
+    *out = c;
+    return LG_OK;
+}
+
+lg_status lg_config_format(const lg_config *cfg, char *buf, uint64_t *len) {
+    if (!cfg || !len || cfg->recursive_steps < 1 || cfg->recursive_steps > LG_MAX_STEPS || cfg->initial_log_m > 63 ||
+        cfg->initial_log_n > 63)
+        return LG_ERR_INVALID_ARGUMENT;
+    std::string s = "recursive_steps = " + std::to_string(cfg->recursive_steps) + "\n";
+    s += "initial_dims = " + std::to_string(1ull << cfg->initial_log_m) + " " +
+         std::to_string(1ull << cfg->initial_log_n) + "\n";
+    s += "initial_k = " + std::to_string(cfg->initial_k) + "\n";
+    s += "dims =";
+    for (uint32_t i = 0; i < cfg->recursive_steps; ++i) {
+        if (cfg->log_m[i] > 63 || cfg->log_n[i] > 63) return LG_ERR_INVALID_ARGUMENT;
+        s += (i ? ", " : " ") + std::to_string(1ull << cfg->log_m[i]) + " " + std::to_string(1ull << cfg->log_n[i]);
+    }
+    s += "\nks =";
+    for (uint32_t i = 0; i < cfg->recursive_steps; ++i) s += " " + std::to_string(cfg->ks[i]);
+    s += "\n";
+    const uint64_t need = s.size() + 1;  // with the terminating NUL
+    if (!buf || *len < need) {
+        const bool ask = !buf;
+        *len = need;
+        return ask ? LG_OK : LG_ERR_INVALID_ARGUMENT;
+    }
+    std::memcpy(buf, s.c_str(), need);
+    *len = need;
+    return LG_OK;
+}
+
 lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
     if (!out) return LG_ERR_INVALID_ARGUMENT;
     *out = nullptr;

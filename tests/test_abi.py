@@ -170,3 +170,34 @@ def test_no_gpu_fails_loudly(lg):
     with pytest.raises(lg.LigeritoError) as e:
         lg.Context(0)
     assert e.value.status == 7
+
+
+def test_config_text_round_trip(lg):
+    # the hard-coded configs (src/config.rs:6-134) and generated ones survive
+    # text and back; the text of config 24 reads as expected
+    for cfg in [lg.hardcoded_config_20(), lg.hardcoded_config_24()] + [lg.config_for_size(L) for L in (16, 19, 22, 28)]:
+        txt = lg.config_to_text(cfg)
+        back = lg.config_from_text(txt)
+        assert back == cfg and lg.config_to_text(back) == txt
+    txt = lg.config_to_text(lg.hardcoded_config_24())
+    assert "initial_dims = 262144 64" in txt and "dims = 16384 16, 1024 16" in txt and "ks = 4 4" in txt
+    # comments, blank lines, spacing and key order are free
+    alt = "# config 24\n\nks = 4 4\ndims=16384 16 ,1024 16  # two steps\ninitial_k=6\n" \
+          "recursive_steps = 2\n  initial_dims =262144 64\n"
+    assert lg.config_from_text(alt) == lg.hardcoded_config_24()
+
+
+@pytest.mark.parametrize("bad", [
+    "",                                                                       # nothing
+    "recursive_steps = 1\ninitial_dims = 256 16\ninitial_k = 4\ndims = 64 4\n",  # no ks
+    "recursive_steps = 1\ninitial_dims = 250 16\ninitial_k = 4\ndims = 64 4\nks = 2\n",  # not a power of two
+    "recursive_steps = 2\ninitial_dims = 256 16\ninitial_k = 4\ndims = 64 4\nks = 2\n",  # too few steps
+    "recursive_steps = 1\ninitial_dims = 256 16\ninitial_k = 4\ndims = 64 4\nks = 2\nks = 2\n",  # repeated key
+    "recursive_steps = 1\ninitial_dims = 256 16\ninitial_k = x\ndims = 64 4\nks = 2\n",  # not a number
+    "recursive_steps = 1\ninitial_dims = 256 16\ninitial_k = 4\ndims = 64 4\nks = 2\ncolour = 3\n",  # unknown key
+    "recursive_steps 1\n",                                                    # no '='
+])
+def test_config_text_errors(lg, bad):
+    with pytest.raises(lg.LigeritoError) as e:
+        lg.config_from_text(bad)
+    assert e.value.status == 2  # LG_ERR_INVALID_CONFIG
