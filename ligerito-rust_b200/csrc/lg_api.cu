@@ -471,16 +471,22 @@ void induce_dev(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *d_rows, uint
 }
 
 // host rows / queries (verifier, kernel-level API) -> induce_dev
-uint32_t induce_host_rows(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *rows, size_t nrows,
-                          const uint32_t *vch, uint32_t nch, const std::vector<uint64_t> &q, uint32_t alpha,
-                          uint32_t *d_out) {
+// The enforced sum arrives in pinned memory, valid after sc.finish().
+const uint32_t *induce_host_rows_later(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *rows, size_t nrows,
+                                       const uint32_t *vch, uint32_t nch, const std::vector<uint64_t> &q,
+                                       uint32_t alpha, uint32_t *d_out) {
     const uint32_t *d_rows = sc.upload(rows, nrows << nch);
     const uint64_t *d_q = sc.upload(q.data(), q.size());
     uint32_t *d_sum = static_cast<uint32_t *>(sc.dev(16));
     induce_dev(c, sc, n, d_rows, (uint32_t)nrows, vch, nch, d_q, alpha, d_out, d_sum);
-    uint32_t sum = 0;
-    d2h(c, &sum, d_sum, 4);
-    return sum;
+    return sc.download_later(d_sum, 1);
+}
+uint32_t induce_host_rows(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *rows, size_t nrows,
+                          const uint32_t *vch, uint32_t nch, const std::vector<uint64_t> &q, uint32_t alpha,
+                          uint32_t *d_out) {
+    const uint32_t *h = induce_host_rows_later(c, sc, n, rows, nrows, vch, nch, q, alpha, d_out);
+    sync(c);
+    return *h;
 }
 
 // partial_eval by any number of challenges (host rs, or device d_rs),
@@ -710,8 +716,13 @@ bool opening_ok_host(const std::vector<uint8_t> &root, const lg::Opening &o, siz
 // tree; every proof node the opening consumes present and 32 bytes), which
 // are exactly the cases where the host walk neither panics nor meets a
 // sibling of another length.  Anything else takes the host walk.
-bool opening_ok(lg_ctx *c, Scratch &sc, const std::vector<uint8_t> &root, const lg::Opening &o, size_t depth,
-                const std::vector<uint64_t> &q) {
+// Checks whose failure is a verifier panic wherever it is found are queued
+// on the device as the verifier goes and decided by finalizers at the next
+// synchronisation (sc.finish(), which throws their panic).  Nothing the
+// verifier computes depends on them, so deciding them late gives the same
+// outcome as the reference's early panics.
+void check_opening(lg_ctx *c, Scratch &sc, const std::vector<uint8_t> &root, const lg::Opening &o, size_t depth,
+                   const std::vector<uint64_t> &q) {
     const size_t nq = q.size();
     bool fast = nq >= 1 && nq <= 256 && o.rows.size() >= nq && depth >= 1 && depth <= 63;
     const size_t ncols = fast ? o.rows.len(0) : 0;
@@ -724,7 +735,10 @@ bool opening_ok(lg_ctx *c, Scratch &sc, const std::vector<uint8_t> &root, const 
         fast = o.merkle.size() >= refs.size();
         for (size_t j = 0; fast && j < refs.size(); ++j) fast = o.merkle.len(j) == 32;
     }
-    if (!fast) return opening_ok_host(root, o, depth, q);
+    if (!fast) {
+        if (!opening_ok_host(root, o, depth, q)) throw VerifyPanic{};
+        return;
+    }
     const uint32_t *d_rows = sc.upload(o.rows.data.data(), nq * ncols);
     const uint64_t *d_q = sc.upload(q.data(), nq);
     const uint32_t *d_proof = refs.empty() ? nullptr
@@ -732,9 +746,11 @@ bool opening_ok(lg_ctx *c, Scratch &sc, const std::vector<uint8_t> &root, const 
                                                        8 * refs.size());
     uint32_t *d_out = static_cast<uint32_t *>(sc.dev(9 * 4));
     CK(c, lgk::opening_check(c->L, d_rows, (uint32_t)ncols, d_q, (uint32_t)nq, d_proof, (uint32_t)depth, d_out));
-    uint32_t out[9];
-    d2h(c, out, d_out, sizeof out);
-    return out[8] == 1 && root.size() == 32 && std::memcmp(out, root.data(), 32) == 0;
+    const uint32_t *h = sc.download_later(d_out, 9);
+    const std::vector<uint8_t> *rp = &root;
+    sc.finalizers.push_back([h, rp]() {
+        if (!(h[8] == 1 && rp->size() == 32 && std::memcmp(h, rp->data(), 32) == 0)) throw VerifyPanic{};
+    });
 }
 
 std::vector<uint32_t> dense(const lg::Opening &o, size_t want_rows, size_t want_len) {
@@ -801,9 +817,10 @@ void ligero_verify_dev(lg_ctx *c, Scratch &sc, const std::vector<uint64_t> &q, c
     CK(c, cudaMemsetAsync(d_bad, 0, 4, c->stream));
     CK(c, lgk::ligero_check(c->L, d_rows, d_off, (uint32_t)nrows, d_gr, (uint32_t)gr.size(), d_yr, nv, d_q,
                             sks.data(), d_bad));
-    uint32_t bad = 0;
-    d2h(c, &bad, d_bad, 4);
-    if (bad) throw VerifyPanic{};
+    const uint32_t *h = sc.download_later(d_bad, 1);
+    sc.finalizers.push_back([h]() {
+        if (*h != 0) throw VerifyPanic{};
+    });
 }
 
 bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &P) {
@@ -818,7 +835,7 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
     size_t depth = cfg.initial_log_m + log_inv_rate;
     std::vector<uint64_t> q;
     if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};
-    if (!opening_ok(c, sc, P.initial_root, P.initial, depth, q)) throw VerifyPanic{};  // :42-49
+    check_opening(c, sc, P.initial_root, P.initial, depth, q);  // :42-49
     const uint32_t alpha = fs.get_field();
     std::vector<uint32_t> rows = dense(P.initial, s, 1ull << cfg.initial_k);
     std::vector<DBuf> basis;
@@ -826,8 +843,8 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
     basis.emplace_back(c, 4ull << cfg.initial_log_m);
     bvars.push_back(cfg.initial_log_m);
     sep.push_back(1);
-    const uint32_t h1 = induce_host_rows(c, sc, cfg.initial_log_m, rows.data(), s, pe0.data(), cfg.initial_k, q,
-                                         alpha, basis.back().u32());  // :53-60
+    const uint32_t *h1 = induce_host_rows_later(c, sc, cfg.initial_log_m, rows.data(), s, pe0.data(),
+                                                cfg.initial_k, q, alpha, basis.back().u32());  // :53-60
     // SumcheckVerifierInstance::new (src/ligerito.rs:172-192)
     size_t rd = 0;
     auto read_tr = [&]() {
@@ -835,7 +852,12 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
         return P.transcript[rd++];
     };
     std::array<uint32_t, 3> g = read_tr();
-    if ((g[0] ^ g[1]) != h1) throw VerifyPanic{};
+    {
+        const uint32_t e = g[0] ^ g[1];
+        sc.finalizers.push_back([h1, e]() {
+            if (*h1 != e) throw VerifyPanic{};
+        });
+    }
     Quad running = quad_from_evals(g[0], g[1], g[2]);
     absorb3(fs, g);  // :67
     std::vector<uint32_t> ris;
@@ -857,7 +879,7 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
             fs.absorb_u32s(P.yr.data(), P.yr.size());
             depth = cfg.log_m[i] + log_inv_rate;
             if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};
-            if (!opening_ok(c, sc, root, P.final_, depth, q)) throw VerifyPanic{};
+            check_opening(c, sc, root, P.final_, depth, q);
             ligero_verify_dev(c, sc, q, P.final_, P.yr, rs);
             const uint32_t final_r = fs.get_field();  // :114
             const size_t yl = P.yr.size();
@@ -870,7 +892,8 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
             while ((1ull << k) < fe.size()) ++k;
             const uint32_t sum = eval_quad(running, final_r);
             ris.push_back(final_r);
-            std::vector<uint32_t> acc(fe.size(), 0), part(fe.size());
+            std::vector<uint32_t> acc(fe.size(), 0);
+            std::vector<const uint32_t *> parts;
             for (size_t bi = 0; bi < basis.size(); ++bi) {  // evaluate_basis_polys_partially :257-280
                 const uint32_t nv = bvars[bi];
                 size_t npts, first;
@@ -883,10 +906,12 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
                 if (npts == 0 || npts > nv || (1ull << (nv - npts)) != fe.size()) throw VerifyPanic{};
                 DBuf d(c, 4ull << (nv - npts));
                 partial_eval_dev(c, basis[bi].u32(), nv, ris.data() + first, (uint32_t)npts, d.u32());
-                d2h(c, part.data(), d.p, 4 * part.size());
-                for (size_t j = 0; j < acc.size(); ++j)
-                    acc[j] ^= bi == 0 ? part[j] : lg::gf_mul(sep[bi], part[j]);
+                parts.push_back(sc.download_later(d.u32(), fe.size()));
             }
+            sc.finish();  // also decides the queued checks
+            for (size_t bi = 0; bi < parts.size(); ++bi)
+                for (size_t j = 0; j < acc.size(); ++j)
+                    acc[j] ^= bi == 0 ? parts[bi][j] : lg::gf_mul(sep[bi], parts[bi][j]);
             uint32_t dot = 0;
             for (size_t j = 0; j < fe.size(); ++j) dot ^= lg::gf_mul(fe[j], acc[j]);
             return dot == sum;
@@ -895,15 +920,20 @@ bool verify_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const lg::Proof &
         fs.absorb(P.recursive_roots[i + 1].data(), P.recursive_roots[i + 1].size());  // :122
         depth = cfg.log_m[i] + log_inv_rate;
         if (!fs.get_distinct_queries(1ull << depth, s, q)) throw VerifyPanic{};  // :126
-        if (!opening_ok(c, sc, root, P.recursive[i], depth, q)) throw VerifyPanic{};
+        check_opening(c, sc, root, P.recursive[i], depth, q);
         const uint32_t al = fs.get_field();  // :345
         std::vector<uint32_t> rr = dense(P.recursive[i], s, 1ull << cfg.ks[i]);
         basis.emplace_back(c, 4ull << cfg.log_m[i]);
         bvars.push_back(cfg.log_m[i]);
-        const uint32_t h = induce_host_rows(c, sc, cfg.log_m[i], rr.data(), s, rs.data(), cfg.ks[i], q, al,
-                                            basis.back().u32());
+        const uint32_t *h = induce_host_rows_later(c, sc, cfg.log_m[i], rr.data(), s, rs.data(), cfg.ks[i], q, al,
+                                                   basis.back().u32());
         g = read_tr();  // introduce_new (src/ligerito.rs:212-220)
-        if ((g[0] ^ g[1]) != h) throw VerifyPanic{};
+        {
+            const uint32_t e = g[0] ^ g[1];
+            sc.finalizers.push_back([h, e]() {
+                if (*h != e) throw VerifyPanic{};
+            });
+        }
         Quad to_glue = quad_from_evals(g[0], g[1], g[2]);
         absorb3(fs, g);
         const uint32_t beta = fs.get_field();  // :358
