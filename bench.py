@@ -100,6 +100,63 @@ class ClockSampler:
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
 
 
+# Fixed algorithmic units (set once): 16 INT32 operations per GF(2^32)
+# multiplication (a multiply-by-constant from table lookups or bit slices),
+# 800 per BLAKE3 compression (7 rounds x 8 G x 14 operations + 16 output
+# XORs), 8 shared-memory wavefronts per 32 table multiplications.
+INT_OPS_PER_MULT, INT_OPS_PER_COMPRESSION = 16, 800
+SERIAL_KERNELS = ("fs_", "opening_check", "ligero_check")
+
+
+def kernel_rooflines(stats, work, hbm_peak_gbs, peak_kind, pipes):
+    """Per-kernel roofline of one proof.  For each kernel: its compulsory HBM
+    bytes over the measured copy bandwidth, its INT32 operations over the
+    measured LOP3 rate (the integer logic pipe, which binds the table
+    multiplies and BLAKE3), the table lookups' shared-memory wavefronts over
+    the measured conflict-free load rate; the binding time is the largest,
+    and frac = binding time / measured time.  The headline object keeps the
+    HBM form for the dominant kernel."""
+    int_peak = pipes.get("lop3") or None
+    lds_peak = pipes.get("lds") or None
+    per = {}
+    for name, (n, ms) in sorted(stats.items(), key=lambda kv: -kv[1][1]):
+        b, m, c = work.get(name, (0.0, 0.0, 0.0))
+        t = ms / 1e3
+        int_ops = INT_OPS_PER_MULT * m + INT_OPS_PER_COMPRESSION * c
+        t_hbm = b / (hbm_peak_gbs * 1e9)
+        t_int = int_ops / int_peak if int_peak else 0.0
+        t_lds = (m * 8 / 32) / lds_peak if (lds_peak and name.startswith(("fft", "ifft", "fold", "rs_scale", "axpy",
+                                                                           "induce_main", "eval013"))) else 0.0
+        bound = max((t_hbm, "hbm"), (t_int, "int32"), (t_lds, "smem_lookups"))
+        row = {"launches": n, "ms": round(ms, 4), "ms_per_launch": round(ms / n, 5),
+               "hbm_bytes": int(b), "gf_mults": int(m), "blake3_compressions": int(c),
+               "hbm_gbs": round(b / t / 1e9, 1) if t > 0 else None,
+               "frac_hbm": round(t_hbm / t, 4) if t > 0 else None,
+               "frac_int32": round(t_int / t, 4) if t > 0 and int_peak else None}
+        if t_lds:
+            row["frac_smem_lookups"] = round(t_lds / t, 4)
+        if name.startswith(SERIAL_KERNELS) or bound[0] == 0.0:
+            row["bound"], row["frac"] = "latency (serial chain)", None
+        else:
+            row["bound"], row["frac"] = bound[1], round(bound[0] / t, 4) if t > 0 else None
+        per[name] = row
+    top = max(stats.items(), key=lambda kv: kv[1][1])[0]
+    r = per[top]
+    avg_s = r["ms_per_launch"] / 1e3
+    achieved = r["hbm_bytes"] / r["launches"] / avg_s / 1e9
+    return {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": hbm_peak_gbs,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm_peak_gbs, 4),
+            "traffic": _traffic_per_launch(top), "avg_launch_ms": round(r["ms_per_launch"], 4),
+            "binding": {"bound": r["bound"], "frac": r["frac"]},
+            "int32_peak_gops": round(int_peak / 1e9, 1) if int_peak else None,
+            "int32_peak_kind": "measured in this run (LOP3 throughput microkernel, lg_measure_pipe_peaks)",
+            "smem_lookup_peak_gwavefronts": round(lds_peak / 1e9, 1) if lds_peak else None,
+            "pipe_peaks_gops": {k: round(v / 1e9, 1) for k, v in pipes.items()},
+            "units": "int32 ops = 16 per GF(2^32) mult + 800 per BLAKE3 compression; "
+                     "smem wavefronts = 8 per 32 table mults",
+            "per_kernel": per}
+
+
 def cpu_baseline(log_size: int = 24, seed: int = 1, threads: int | None = None):
     """The oracle (C restatement of the reference CPU prover) on host cores:
     one full proof of the same workload."""
@@ -165,6 +222,7 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     ctx = lg.Context(dev)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=f"cuda:{dev}")
+    pipes = lg.measure_pipe_peaks(dev)
     cfg = lg.hardcoded_config_24()
     seed = 1 + rank  # independent replica inputs; rank 0 proves the seed-1 workload
     poly = lg.splitmix_coeffs_device(seed, cfg.poly_len, ctx)
@@ -232,42 +290,17 @@ def run_ours(args):
         h2d.append(a.elapsed_time(b))
     torch.cuda.synchronize()
 
-    # --- roofline of the dominant kernel: per-kernel CUDA events on the
-    #     launching stream (a separate pass, not the timed one)
+    # --- rooflines: per-kernel CUDA events on the launching stream (a
+    #     separate pass, not the timed one) and each kernel's algorithmic
+    #     work as the library books it per launch
     ctx.set_kernel_timing(True)
     ctx.reset_kernel_stats()
     lg.prover(cfg, poly, ctx)
     stats = ctx.kernel_stats()
+    work = ctx.kernel_work()
     ctx.set_kernel_timing(False)
-    top = max(stats.items(), key=lambda kv: kv[1][1])
-    name, (n_launch, tot_ms) = top
-    avg_s = tot_ms / n_launch / 1e3
-    # fft_pass at L=18 on the 64-column first-round matrix: every launch
-    # reads and writes the whole 4 x 2^18 x 64 word matrix once and does K
-    # stages of 4 x 64 x 2^17 butterflies (one GF multiply each)
-    algo_bytes = 2 * 4 * (4 << 18) * 64 if name.startswith("fft_pass_L18") else None
     peak, peak_kind = _peaks()
-    achieved = (algo_bytes / avg_s / 1e9) if algo_bytes else None
-    k_stages = int(name.split("_K")[1].split("_")[0]) if name.startswith("fft_pass_L18_K") else None
-    mults = (64 * 4 * (1 << 17) * k_stages) if k_stages else None  # GF mults per launch
-    roofline = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1) if achieved else None,
-                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": round(achieved / peak, 4) if achieved else None,
-                "traffic": _traffic_per_launch(name), "avg_launch_ms": round(avg_s * 1e3, 4),
-                "gf_mults_per_launch": mults,
-                "gf_mults_per_s": round(mults / avg_s, 1) if mults else None,
-                "kernel_ms": {k: round(v[1], 4) for k, v in sorted(stats.items(), key=lambda kv: -kv[1][1])}}
-    if mults:
-        # The FFT passes are not HBM-bound: every multiply is 8 table
-        # lookups in shared memory, and a conflict-free warp lookup is one
-        # 128-byte wavefront, of which an SM serves one per clock.
-        sm_hz = float((clocks or {}).get("sm_mhz") or 1965.0) * 1e6
-        wf = mults / 32 * 8 / avg_s / 1e9
-        wf_peak = 148 * sm_hz / 1e9
-        roofline["secondary"] = {"bound": "shared-memory table lookups", "achieved": round(wf, 1),
-                                 "peak": round(wf_peak, 1), "unit": "G wavefronts/s",
-                                 "frac": round(wf / wf_peak, 4),
-                                 "peak_basis": "148 SMs x 1 wavefront/clock at the sampled SM clock"}
+    roofline = kernel_rooflines(stats, work, peak, peak_kind, pipes)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -296,6 +329,64 @@ def run_ours(args):
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def run_prove_large(args):
+    """Config 3: one 2^28 proof (1 GiB of coefficients, SplitMix64 seed 2,
+    the generated config), device-resident input, CUDA events per proof;
+    then one proof from pinned host memory (e2e) and a kernel-timing pass
+    with every kernel's roofline."""
+    import torch
+
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as g
+
+    lg = g.load_package()
+    ctx = lg.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device="cuda:0")
+    pipes = lg.measure_pipe_peaks(0)
+    L = 28
+    cfg = lg.config_for_size(L)
+    poly = lg.splitmix_coeffs_device(2, cfg.poly_len, ctx)
+    for _ in range(max(1, args.warmup)):
+        lg.prover(cfg, poly, ctx)
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(0) as clk:
+        for _ in range(max(1, args.steps)):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            proof = lg.prover(cfg, poly, ctx)
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+    clocks = clk.summary()
+    pb = proof.to_bytes()
+    host = torch.empty(cfg.poly_len, dtype=torch.int32, pin_memory=True)
+    host.copy_(poly.cpu())
+    host_np = host.numpy().view("uint32")
+    lg.prover(cfg, host_np, ctx)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    pb2 = lg.prover(cfg, host_np, ctx).to_bytes()
+    b.record(stream)
+    b.synchronize()
+    assert pb2 == pb
+    ctx.set_kernel_timing(True)
+    ctx.reset_kernel_stats()
+    lg.prover(cfg, poly, ctx)
+    stats, work = ctx.kernel_stats(), ctx.kernel_work()
+    ctx.set_kernel_timing(False)
+    peak, peak_kind = _peaks()
+    print(json.dumps({"workload": "prove28", "metric": "prove ms at 2^28 (generated config, seed 2)",
+                      "value": round(statistics.median(times), 3), "unit": "ms", "steps": len(times),
+                      "warmup": max(1, args.warmup), "higher_is_better": False, "min_ms": round(min(times), 3),
+                      "proof_bytes": len(pb), "proof_sha256": __import__("hashlib").sha256(pb).hexdigest(),
+                      "e2e": {"value": round(a.elapsed_time(b), 3), "unit": "ms",
+                              "h2d_bytes_per_step": 4 * cfg.poly_len, "d2h_bytes_per_step": len(pb2)},
+                      "clocks": clocks, "data": "synthetic (SplitMix64 seed 2)",
+                      "roofline": kernel_rooflines(stats, work, peak, peak_kind, pipes)}), flush=True)
 
 
 def run_micro(args):
@@ -336,10 +427,14 @@ def run_micro(args):
     ctx.set_kernel_timing(True)
     ctx.reset_kernel_stats()
     run()
-    stats = ctx.kernel_stats()
+    stats, work = ctx.kernel_stats(), ctx.kernel_work()
+    ctx.set_kernel_timing(False)
+    peak, peak_kind = _peaks()
     print(json.dumps({"workload": w, "metric": metric, "value": round(statistics.median(times), 4) if times else None,
                       "unit": "ms", "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-                      "kernel_ms": {k: [v[0], round(v[1], 4)] for k, v in stats.items()}}), flush=True)
+                      "data": "synthetic (SplitMix64 seed 1)",
+                      "roofline": kernel_rooflines(stats, work, peak, peak_kind, lg.measure_pipe_peaks(0))}),
+          flush=True)
 
 
 def run_verify(args):
@@ -541,7 +636,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="prove24",
-                    choices=["prove24", "commit24", "fft16", "fft20", "fft22", "ifft16", "ifft20", "ifft22",
+                    choices=["prove24", "prove28", "commit24", "fft16", "fft20", "fft22", "ifft16", "ifft20", "ifft22",
                              "batch64", "serve", "verify24"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests per rate")
@@ -556,6 +651,8 @@ def main():
         run_serve(args)
     elif args.workload == "verify24":
         run_verify(args)
+    elif args.workload == "prove28":
+        run_prove_large(args)
     elif args.workload != "prove24":
         run_micro(args)
     else:

@@ -97,7 +97,41 @@ lg_status lg_ctx_set_kernel_timing(lg_ctx *ctx, int enabled);
 lg_status lg_ctx_kernel_stats(lg_ctx *ctx, uint32_t index, char *name, size_t name_cap,
                               uint64_t *launches, double *total_ms); /* INVALID_ARGUMENT past end */
 lg_status lg_ctx_reset_kernel_stats(lg_ctx *ctx);
+/* Algorithmic work of the timed launches of entry `index` (the same order as
+ * lg_ctx_kernel_stats), summed over its launches: compulsory HBM bytes (every
+ * input read once, every output written once), GF(2^32) multiplications and
+ * BLAKE3 compressions.  The roofline of each kernel divides these by the
+ * device's peak rates.  No reference counterpart (measurement only). */
+lg_status lg_ctx_kernel_work(lg_ctx *ctx, uint32_t index, double *hbm_bytes, double *gf_mults,
+                             double *blake3_compressions);
 uint64_t lg_ctx_device_bytes_in_use(const lg_ctx *ctx);
+/* Device bytes a context keeps between calls (its arena, reserved on its
+ * first call, and its FFT tables), and the bytes of the code / twiddle
+ * tables that all contexts on a device share (ReedSolomonEncoding::new's
+ * twiddles and pis per size, src/reed_solomon.rs:49-64), held while a
+ * context on that device exists. */
+uint64_t lg_ctx_device_bytes_cached(const lg_ctx *ctx);
+uint64_t lg_device_table_bytes(int device);
+
+/* Peak rates of the device's integer pipes and shared memory, measured by
+ * throughput microkernels on `device`: rates[k] for k < count (k an
+ * lg_pipe), in instructions per second over the whole device.  LG_PIPE_LDS
+ * counts warp-wide conflict-free shared loads (wavefronts); LG_PIPE_LOP3_IMAD
+ * counts both instructions of an interleaved pair, so it shows whether the
+ * logic and multiply-add pipes issue together.  These are the denominators of
+ * the integer rooflines.  No reference counterpart (measurement only). */
+typedef enum lg_pipe {
+    LG_PIPE_LOP3 = 0,      /* 3-input logic (XOR) */
+    LG_PIPE_IADD = 1,      /* 32-bit add */
+    LG_PIPE_PRMT = 2,      /* byte permute */
+    LG_PIPE_SHF = 3,       /* funnel shift */
+    LG_PIPE_IMAD = 4,      /* 32-bit multiply-add, low half */
+    LG_PIPE_IMAD_HI = 5,   /* 32-bit multiply-add, high half */
+    LG_PIPE_LOP3_IMAD = 6, /* LOP3 and IMAD interleaved */
+    LG_PIPE_LDS = 7,       /* conflict-free 32-bit shared-memory loads */
+    LG_PIPE_COUNT = 8
+} lg_pipe;
+lg_status lg_measure_pipe_peaks(int device, double *rates, uint32_t count);
 
 /* ------------------------------------------------------------ prove/verify */
 /* prover::<BinaryElem32>(config, poly), src/prover.rs:15.  `poly` holds
@@ -138,11 +172,20 @@ lg_status lg_server_create(int device, uint64_t hbm_budget_bytes, uint32_t worke
 lg_status lg_server_submit(lg_server *srv, const lg_config *cfg, const uint32_t *poly, uint64_t len,
                            int poly_on_device, int copy_input, uint64_t *ticket);
 /* timeout_ms < 0 waits forever; LG_ERR_TIMEOUT leaves the ticket valid.
- * latency_ms = submit -> done, queue_ms = submit -> start (may be NULL). */
+ * latency_ms = submit -> done, queue_ms = submit -> start (may be NULL).
+ * A ticket's result is handed out once: of several threads waiting on one
+ * ticket, the first to wake takes it and the others get
+ * LG_ERR_INVALID_ARGUMENT, as does any later wait on it. */
 lg_status lg_server_wait(lg_server *srv, uint64_t ticket, int64_t timeout_ms, lg_proof **proof,
                          double *latency_ms, double *queue_ms);
 lg_status lg_server_stats(lg_server *srv, uint64_t *completed, uint64_t *queued, uint64_t *in_flight_bytes);
 void lg_server_destroy(lg_server *srv); /* finishes queued work first */
+/* Proves one polynomial of each of the `count` configs on every worker at
+ * once (inputs generated on the device), so that every worker's context has
+ * its tables for those sizes and the device memory pool has grown to all
+ * workers proving the largest size together: requests that follow pay none
+ * of these first-use costs.  Waits for the proofs and discards them. */
+lg_status lg_server_warm(lg_server *srv, const lg_config *cfgs, uint32_t count);
 /* count proofs on `workers` concurrent contexts; out[i] as lg_prove */
 lg_status lg_prove_batch(int device, uint32_t workers, const lg_config *cfgs, const uint32_t *const *polys,
                          const uint64_t *lens, int polys_on_device, uint32_t count, lg_proof **out);
@@ -221,19 +264,26 @@ lg_status lg_merkle_verify(const uint8_t *root, const uint8_t *proof, uint64_t n
  * call above, not a reference interface).
  *
  * Inputs and outputs are the caller's device buffers: d_rows (nrows x
- * 2^nch words, row-major), d_queries (nrows sorted row indices),
- * d_basis_out (2^n words), d_enforced_sum (1 word); v_challenges stays on
- * the host.  Work is queued on `stream` (a cudaStream_t; NULL = the legacy
- * default stream) and the call returns without waiting for it.
+ * 2^nch words, row-major), d_queries (nrows sorted row indices, each below
+ * 2^32: the device reads their low 32 bits, so larger values, which the
+ * regular call rejects with LG_ERR_INVALID_ARGUMENT, give undefined
+ * results here), d_basis_out (2^n words), d_enforced_sum (1 word);
+ * v_challenges stays on the host.  Work is queued on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream) behind the work already
+ * on it, and the call returns without waiting for it.
  *
  * Scratch comes from one fixed array of LG_NOALLOC_SCRATCH_BYTES in device
- * memory, reserved when the library loads and held by every GPU that loads
- * it until the process exits.  Limit: nrows <= 256 and n <= 20 (anything
- * larger returns LG_ERR_EXCEEDS_STATIC_SCRATCH and queues no work).  The
- * first call on a device looks up that device's copy of the array, so it
- * should come before any stream capture.  All calls share the array: calls
- * whose work overlaps on the GPU race on it, so order them on one stream or
- * wait between them. */
+ * memory, held by every GPU that has loaded it until the process exits.
+ * Limit: nrows <= 256 and n <= 20 (anything larger returns
+ * LG_ERR_EXCEEDS_STATIC_SCRATCH and queues no work).  The array lives in
+ * its own code module, which the CUDA runtime loads lazily: the first call
+ * on each device loads that module and reserves the array there (the
+ * driver allocates it, which can synchronise the device) and looks up the
+ * array's device address.  Make one warm-up call on each device at
+ * start-up, before any stream capture and before latency-critical work;
+ * later calls allocate nothing.  All calls share the array: calls whose
+ * work overlaps on the GPU race on it, so order them on one stream or wait
+ * between them. */
 #define LG_NOALLOC_SCRATCH_BYTES (4u << 20)
 lg_status lg_induce_sumcheck_poly_noalloc(void *stream, uint32_t n, const uint32_t *d_rows, uint32_t nrows,
                                           const uint32_t *v_challenges, uint32_t nch,

@@ -99,7 +99,12 @@ def _load() -> ctypes.CDLL:
         "lg_ctx_set_kernel_timing": (i32, [P, i32]),
         "lg_ctx_kernel_stats": (i32, [P, u32, ctypes.c_char_p, ctypes.c_size_t, P, P]),
         "lg_ctx_reset_kernel_stats": (i32, [P]),
+        "lg_ctx_kernel_work": (i32, [P, u32, P, P, P]),
+        "lg_measure_pipe_peaks": (i32, [i32, P, u32]),
         "lg_ctx_device_bytes_in_use": (u64, [P]),
+        "lg_ctx_device_bytes_cached": (u64, [P]),
+        "lg_device_table_bytes": (u64, [i32]),
+        "lg_server_warm": (i32, [P, P, u32]),
         "lg_prove": (i32, [P, P, P, u64, i32, P]),
         "lg_verify": (i32, [P, P, P, P]),
         "lg_proof_serialize": (i32, [P, P, P]),
@@ -384,12 +389,36 @@ class Context:
             i += 1
         return out
 
+    def kernel_work(self) -> dict:
+        """name -> (compulsory HBM bytes, GF(2^32) multiplications, BLAKE3
+        compressions) of the timed launches, the same keys as kernel_stats."""
+        out, i = {}, 0
+        names = list(self.kernel_stats())
+        b, m, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        while i < len(names) and lib.lg_ctx_kernel_work(self.handle, i, ctypes.byref(b), ctypes.byref(m),
+                                                        ctypes.byref(c)) == 0:
+            out[names[i]] = (float(b.value), float(m.value), float(c.value))
+            i += 1
+        return out
+
     def reset_kernel_stats(self) -> None:
         _check(lib.lg_ctx_reset_kernel_stats(self.handle), self)
 
     @property
     def device_bytes_in_use(self) -> int:
         return int(lib.lg_ctx_device_bytes_in_use(self.handle))
+
+
+PIPES = ("lop3", "iadd", "prmt", "shf", "imad", "imad_hi", "lop3_imad", "lds")
+
+
+def measure_pipe_peaks(device: int = 0) -> dict:
+    """Peak instruction rates of the device's integer pipes and of
+    conflict-free shared-memory loads (lg_measure_pipe_peaks), per second
+    over the whole device."""
+    rates = (ctypes.c_double * len(PIPES))()
+    _check(lib.lg_measure_pipe_peaks(device, rates, len(PIPES)))
+    return {k: float(v) for k, v in zip(PIPES, rates)}
 
 
 _default_ctx: dict = {}
@@ -706,6 +735,13 @@ class Server:
         self._keep.pop(ticket, None)
         _check(st)
         return FinalizedLigeritoProof(h), float(lat.value), float(q.value)
+
+    def warm(self, configs: Sequence[ProverConfig]) -> None:
+        """One proof of each config on every worker at once (lg_server_warm):
+        later requests pay no first-use costs."""
+        n = len(configs)
+        cfgs = (LgConfig * n)(*[c.to_c() for c in configs])
+        _check(lib.lg_server_warm(self.handle, cfgs, n))
 
     def stats(self) -> dict:
         c, q, b = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()

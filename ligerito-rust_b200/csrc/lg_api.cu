@@ -10,6 +10,7 @@
 #include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -30,6 +31,18 @@ struct Code {  // ReedSolomonEncoding::new(m, 4m) tables, src/reed_solomon.rs:49
     uint32_t *pis = nullptr;  // compute_pis(m, eval_sk_at_vks(m)): m words
 };
 
+// The code and twiddle tables depend only on the size, so every context on
+// a device shares one copy (a server's workers would otherwise each build
+// and hold their own).  They live while a context on the device does.
+struct DeviceTables {
+    int contexts = 0;
+    uint64_t bytes = 0;
+    std::map<uint32_t, Code> codes;        // by log_m
+    std::map<uint32_t, uint32_t *> ffttw;  // by log_n, plain fft twiddles
+};
+std::mutex g_tables_mu;
+std::map<int, DeviceTables> g_tables;
+
 }  // namespace
 
 struct lg_ctx {
@@ -40,8 +53,6 @@ struct lg_ctx {
     lgk::Launcher L;
     uint64_t budget = 0, in_use = 0;
     std::string err;
-    std::map<uint32_t, Code> codes;       // by log_m
-    std::map<uint32_t, uint32_t *> ffttw;  // by log_n, plain fft twiddles
     uint8_t *pinned = nullptr;  // staging for small synchronous transfers
     size_t pinned_cap = 0;
     // per-call bump arenas (reset at the start of each prove / verify)
@@ -123,30 +134,50 @@ void d2h(lg_ctx *c, void *dst, const void *src, size_t bytes) {
     std::memcpy(dst, p, bytes);
 }
 
-const Code &get_code(lg_ctx *c, uint32_t log_m) {
-    auto it = c->codes.find(log_m);
-    if (it != c->codes.end()) return it->second;
+// The device's shared tables (created on first use, under the lock; the
+// upload is synchronous, so a table is complete before any context sees it).
+Code get_code(lg_ctx *c, uint32_t log_m) {
+    std::lock_guard<std::mutex> lk(g_tables_mu);
+    DeviceTables &t = g_tables[c->device];
+    auto it = t.codes.find(log_m);
+    if (it != t.codes.end()) return it->second;
     const uint64_t m = 1ull << log_m;
     std::vector<uint32_t> tw((4 * m) - 1), pis(m);
     lg::compute_twiddles(log_m + 2, tw.data());
     lg::compute_pis(m, lg::eval_sk_at_vks(m), pis.data());
     Code code;
     CK(c, cudaMalloc(&code.tw, tw.size() * 4));
-    CK(c, cudaMalloc(&code.pis, pis.size() * 4));
-    CK(c, cudaMemcpy(code.tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
-    CK(c, cudaMemcpy(code.pis, pis.data(), pis.size() * 4, cudaMemcpyHostToDevice));
-    return c->codes[log_m] = code;
+    if (cudaMalloc(&code.pis, pis.size() * 4) != cudaSuccess) {
+        cudaFree(code.tw);
+        CK(c, cudaErrorMemoryAllocation);
+    }
+    cudaError_t e = cudaMemcpy(code.tw, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(code.pis, pis.data(), pis.size() * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(code.tw);
+        cudaFree(code.pis);
+        CK(c, e);
+    }
+    t.bytes += (tw.size() + pis.size()) * 4;
+    return t.codes[log_m] = code;
 }
 
 const uint32_t *get_fft_tw(lg_ctx *c, uint32_t log_n) {
-    auto it = c->ffttw.find(log_n);
-    if (it != c->ffttw.end()) return it->second;
+    std::lock_guard<std::mutex> lk(g_tables_mu);
+    DeviceTables &t = g_tables[c->device];
+    auto it = t.ffttw.find(log_n);
+    if (it != t.ffttw.end()) return it->second;
     std::vector<uint32_t> tw((1ull << log_n) - 1);
     lg::compute_twiddles(log_n, tw.data());
     uint32_t *d = nullptr;
     CK(c, cudaMalloc(&d, tw.size() * 4));
-    CK(c, cudaMemcpy(d, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice));
-    return c->ffttw[log_n] = d;
+    cudaError_t e = cudaMemcpy(d, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        CK(c, e);
+    }
+    t.bytes += tw.size() * 4;
+    return t.ffttw[log_n] = d;
 }
 
 // ------------------------------------------------------------- scratch
@@ -163,8 +194,9 @@ struct Scratch {
     std::vector<std::function<void()>> finalizers;
     struct Deferred { uint8_t *h; const void *d; size_t bytes; };
     std::vector<Deferred> deferred;
+    static constexpr size_t kPin = 8u << 20, kDevArena = 32u << 20;
     explicit Scratch(lg_ctx *ctx) : c(ctx) {
-        constexpr size_t kPin = 8u << 20, kDev = 32u << 20;
+        constexpr size_t kDev = kDevArena;
         if (!c->pin_arena) {
             CK(c, cudaMallocHost((void **)&c->pin_arena, kPin));
             c->pin_cap = kPin;
@@ -271,7 +303,7 @@ void rs_encode(lg_ctx *c, const Code &code, const uint32_t *d_poly, uint32_t log
 
 // ligero_commit (src/ligero.rs:70-95) into caller buffers
 void commit_into(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *E, uint32_t *tree) {
-    const Code &code = get_code(c, log_m);
+    const Code code = get_code(c, log_m);
     const uint64_t m = 1ull << log_m, rows = 4 * m;
     {
         DBuf scaled(c, log_m > 6 ? 4ull * n * m : 0);
@@ -304,7 +336,7 @@ Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
 // remains.
 Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_t *d_poly, uint32_t log_m,
                          uint32_t n) {
-    const Code &code = get_code(c, log_m);
+    const Code code = get_code(c, log_m);
     const uint64_t m = 1ull << log_m, rows = 4 * m;
     Witness w;
     w.rows = rows;
@@ -498,14 +530,13 @@ void partial_eval_dev(lg_ctx *c, const uint32_t *d_in, uint32_t log_len, const u
     uint32_t cur = log_len, done = 0, which = 0;
     while (done < k) {
         const uint32_t kk = std::min<uint32_t>(6, k - done);
-        std::vector<uint32_t> gr = d_rs ? std::vector<uint32_t>() : lg::lagrange_basis(rs + done, kk);
         uint32_t *dst;
         if (done + kk == k) dst = d_out;
         else {
             tmp[which] = DBuf(c, 4ull << (cur - kk));
             dst = tmp[which].u32();
         }
-        CK(c, lgk::fold_eq(c->L, src, dst, cur, kk, d_rs ? nullptr : gr.data(), d_rs ? d_rs + done : nullptr));
+        CK(c, lgk::fold_eq(c->L, src, dst, cur, kk, d_rs ? nullptr : rs + done, d_rs ? d_rs + done : nullptr));
         src = dst;
         which ^= 1;
         cur -= kk;
@@ -1184,8 +1215,11 @@ lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
         delete c;
         return LG_ERR_CUDA;
     }
-    if (cudaMalloc((void **)&c->L.dtab, lgk::kDtabSlots * lgk::kDtabWords * 4) != cudaSuccess) {
+    if (cudaMalloc((void **)&c->L.dtab, lgk::kDtabSlots * lgk::kDtabWords * 4) != cudaSuccess ||
+        cudaMalloc((void **)&c->L.tickets, 256) != cudaSuccess || cudaMemset(c->L.tickets, 0, 256) != cudaSuccess) {
         cudaGetLastError();
+        if (c->L.dtab) cudaFree(c->L.dtab);
+        if (c->L.tickets) cudaFree(c->L.tickets);
         cudaStreamDestroy(c->copy_stream);
         cudaStreamDestroy(c->stream);
         delete c;
@@ -1198,6 +1232,10 @@ lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     c->L.stream = c->stream;
+    {
+        std::lock_guard<std::mutex> lk(g_tables_mu);
+        ++g_tables[device].contexts;
+    }
     *out = c;
     return LG_OK;
 }
@@ -1206,12 +1244,20 @@ void lg_ctx_destroy(lg_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    for (auto &kv : c->codes) { cudaFree(kv.second.tw); cudaFree(kv.second.pis); }
-    for (auto &kv : c->ffttw) cudaFree(kv.second);
+    {
+        std::lock_guard<std::mutex> lk(g_tables_mu);
+        auto it = g_tables.find(c->device);
+        if (it != g_tables.end() && --it->second.contexts <= 0) {
+            for (auto &kv : it->second.codes) { cudaFree(kv.second.tw); cudaFree(kv.second.pis); }
+            for (auto &kv : it->second.ffttw) cudaFree(kv.second);
+            g_tables.erase(it);
+        }
+    }
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->pin_arena) cudaFreeHost(c->pin_arena);
     if (c->dev_arena) cudaFree(c->dev_arena);
     if (c->L.dtab) cudaFree(c->L.dtab);
+    if (c->L.tickets) cudaFree(c->L.tickets);
     c->L.release();
     for (auto e : c->copy_ev) if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -1243,13 +1289,37 @@ lg_status lg_ctx_kernel_stats(lg_ctx *c, uint32_t index, char *name, size_t cap,
     if (ms) *ms = it->second.second;
     return LG_OK;
 }
+lg_status lg_ctx_kernel_work(lg_ctx *c, uint32_t index, double *bytes, double *mults, double *comps) {
+    if (!c) return LG_ERR_INVALID_ARGUMENT;
+    lg_status st = guarded(c, [&] { sync(c); c->L.resolve(); });
+    if (st != LG_OK) return st;
+    if (index >= c->L.stats.size()) return LG_ERR_INVALID_ARGUMENT;
+    auto it = c->L.stats.begin();
+    std::advance(it, index);
+    const auto w = c->L.work.find(it->first);
+    const lgk::Launcher::Work none{};
+    const lgk::Launcher::Work &x = w == c->L.work.end() ? none : w->second;
+    if (bytes) *bytes = x.bytes;
+    if (mults) *mults = x.mults;
+    if (comps) *comps = x.comps;
+    return LG_OK;
+}
 lg_status lg_ctx_reset_kernel_stats(lg_ctx *c) {
     if (!c) return LG_ERR_INVALID_ARGUMENT;
     lg_status st = guarded(c, [&] { sync(c); c->L.resolve(); });
     c->L.stats.clear();
+    c->L.work.clear();
     return st;
 }
 uint64_t lg_ctx_device_bytes_in_use(const lg_ctx *c) { return c ? c->in_use : 0; }
+uint64_t lg_ctx_device_bytes_cached(const lg_ctx *c) {
+    return c ? lgk::kDtabSlots * lgk::kDtabWords * 4 + Scratch::kDevArena : 0;
+}
+uint64_t lg_device_table_bytes(int device) {
+    std::lock_guard<std::mutex> lk(g_tables_mu);
+    auto it = g_tables.find(device);
+    return it == g_tables.end() ? 0 : it->second.bytes;
+}
 
 lg_status lg_prove(lg_ctx *c, const lg_config *cfg, const uint32_t *poly, uint64_t len, int on_device,
                    lg_proof **out) {
@@ -1348,7 +1418,7 @@ lg_status lg_rs_encode_cols(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, u
     if (!c || !d_poly || !d_enc || log_m < 1 || log_m > 26 || n == 0) return LG_ERR_INVALID_ARGUMENT;
     return guarded(c, [&] {
         CK(c, cudaSetDevice(c->device));
-        const Code &code = get_code(c, log_m);
+        const Code code = get_code(c, log_m);
         DBuf scaled(c, log_m > 6 ? 4ull * n << log_m : 0);
         rs_encode(c, code, d_poly, log_m, n, d_enc, 4ull << log_m, scaled.u32());
         sync(c);

@@ -31,10 +31,16 @@ void Launcher::begin(const char *, cudaEvent_t *a) {
     cudaEventRecord(*a, stream);
 }
 void Launcher::end(const char *name, cudaEvent_t a) {
+    const Work w = next_work;
+    next_work = {};
     if (!timing) return;
     cudaEvent_t b = get_event();
     cudaEventRecord(b, stream);
     pending.push_back({name, a, b});
+    Work &t = work[name];
+    t.bytes += w.bytes;
+    t.mults += w.mults;
+    t.comps += w.comps;
 }
 void Launcher::resolve() {
     for (auto &p : pending) {
@@ -134,11 +140,13 @@ cudaError_t rs_scale(Launcher &L, const uint32_t *poly, const uint32_t *pis, uin
         // a table costs about as much as 30 general products: worth it from
         // 32 columns on
         const dim3 grid((unsigned)((1ull << log_m) / kScaleRows), (n + kScaleCols - 1) / kScaleCols);
+        L.note(8.0 * n * (1ull << log_m), (double)n * (1ull << log_m));
         LGK_LAUNCH(L, "rs_scale", launch_k(k_rs_scale_tab, grid, 256, 0, L.stream, poly, pis, out, log_m, n));
         return cudaGetLastError();
     }
     const uint64_t total = (uint64_t)n << log_m;
     const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
+    L.note(8.0 * total, (double)total);
     LGK_LAUNCH(L, "rs_scale", launch_k(k_rs_scale, blocks, 256, 0, L.stream, poly, pis, out, log_m, total));
     return cudaGetLastError();
 }
@@ -147,6 +155,7 @@ cudaError_t rs_scale_spread(Launcher &L, const uint32_t *poly, const uint32_t *p
                             uint32_t log_m, uint32_t n) {
     uint64_t total = (uint64_t)n << log_m;
     unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 16);
+    L.note(20.0 * total, (double)total);
     LGK_LAUNCH(L, "rs_scale_spread", launch_k(k_rs_scale_spread, blocks, 256, 0, L.stream, poly, pis, E, log_m, total));
     return cudaGetLastError();
 }
@@ -542,6 +551,13 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
         a.L = log_len; a.d0 = d0; a.log_S = log_len - d0 - K;
         a.log_nvec_p2 = ilog2u(nvec_p2); a.nvec = nvec; a.root_base = root_base;
         const bool tail = a.log_S == 0 && K >= 4 && aligned;
+        {
+            // every vector read (the source once when all Q subtrees share
+            // it) and written once; one product per butterfly and stage
+            const double words = (double)Q * nvec * (1ull << log_len);
+            const double rd = (a.src && src->q_stride == 0) ? words / Q : words;
+            L.note(4.0 * (rd + words), words / 2 * K);
+        }
         if (tail) {
             a.vchunk = std::min<uint32_t>(nvec, 64);
             a.nchunks = (nvec + a.vchunk - 1) / a.vchunk;
@@ -627,12 +643,15 @@ cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint3
                             uint32_t nb, uint32_t *out) {
     if (ncols == 0 || ncols > 256 || nb == 0 || b0 + nb > (ncols + 15) / 16) return cudaErrorInvalidValue;
     const unsigned blocks = (unsigned)((rows + 127) / 128);
+    const uint32_t cols = std::min<uint32_t>(16 * nb, ncols - 16 * b0);
+    L.note((double)rows * (4.0 * cols + (b0 ? 64.0 : 32.0)), 0, (double)rows * nb);
     LGK_LAUNCH(L, "leaf_hash_block", launch_k(k_leaf_block, blocks, 128, 0, L.stream, E, rows, ncols, b0, nb, out, 1u));
     return cudaGetLastError();
 }
 
 cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out) {
     const unsigned blocks = (unsigned)((rows + 127) / 128);
+    L.note((double)rows * (4.0 * ncols + 32.0), 0, (double)rows * ((ncols + 15) / 16));
     LGK_LAUNCH(L, "leaf_hash", launch_k(k_leaf_hash, blocks, 128, 0, L.stream, E, rows, ncols, out, 1u));
     return cudaGetLastError();
 }
@@ -700,32 +719,33 @@ __global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ t
     }
 }
 
-// Narrow layers: a block of 1024 threads takes 2048 consecutive nodes (or
-// the whole layer when it is smaller) and climbs to their common ancestor,
-// one layer per barrier: the first layer up reads the tree, the later ones
-// a shared-memory copy of the layer below.  Every node is also written to
-// the tree.  One launch takes a layer of up to 2^22 nodes eleven layers up
-// (a layer of 2048 or fewer nodes to the root).
-constexpr uint32_t kMerkleBlockNodes = 2048;
-__global__ void __launch_bounds__(1024) k_merkle_block(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
-                                                       uint32_t one) {
-    pdl_begin();
-    // layers in shared memory word-major (word j of node i at [j * stride +
-    // i]): a thread reads its two children's word j as one 8-byte load and
-    // a warp's loads are contiguous
-    __shared__ __align__(16) uint32_t buf_a[8 * (kMerkleBlockNodes / 2)];
-    __shared__ __align__(16) uint32_t buf_b[8 * (kMerkleBlockNodes / 4)];
+// Narrow layers (a layer of at most 2^18 nodes up to the root) in one
+// launch: a block of 256 threads takes 512 consecutive nodes (or the whole
+// layer when it is smaller) and climbs 9 layers, one per barrier -- the
+// first layer up reads the tree, the later ones a shared-memory copy of the
+// layer below -- writing every node to the tree.  Each block then takes a
+// ticket; the last block to finish climbs from the blocks' roots (at most
+// 512 nodes, read back from the tree) to the root.  No block waits for
+// another.
+constexpr uint32_t kNarrowNodes = 512, kNarrowMax = kNarrowNodes * kNarrowNodes;
+
+// Climbs from m nodes (m a power of two, <= 512) of the layer at `off`
+// (nodes first .. first + m - 1 of a layer of n) to their common ancestor;
+// src_tree: the first layer is read from the tree with loads that bypass
+// L1 (nodes other blocks wrote).  Ends with the block synchronised.
+__device__ __forceinline__ void narrow_climb(uint32_t *__restrict__ tree, uint64_t off, uint64_t n, uint64_t first,
+                                             uint32_t m, uint32_t *buf_a, uint32_t *buf_b, uint32_t one) {
     const uint32_t t = threadIdx.x;
-    uint32_t m = (uint32_t)(n_in < kMerkleBlockNodes ? n_in : kMerkleBlockNodes);  // this block's nodes in the layer
-    uint64_t off = in_off, n = n_in, first = blockIdx.x * (uint64_t)m;
     if (t < m / 2) {
         uint32_t l[8], r[8], h[8];
-        load_node(tree + 8 * (off + first + 2 * t), l);
-        load_node(tree + 8 * (off + first + 2 * t + 1), r);
+        const uint4 *pl = reinterpret_cast<const uint4 *>(tree + 8 * (off + first + 2 * t));
+        const uint4 a0 = __ldcg(pl), a1 = __ldcg(pl + 1), b0 = __ldcg(pl + 2), b1 = __ldcg(pl + 3);
+        l[0] = a0.x; l[1] = a0.y; l[2] = a0.z; l[3] = a0.w; l[4] = a1.x; l[5] = a1.y; l[6] = a1.z; l[7] = a1.w;
+        r[0] = b0.x; r[1] = b0.y; r[2] = b0.z; r[3] = b0.w; r[4] = b1.x; r[5] = b1.y; r[6] = b1.z; r[7] = b1.w;
         hash_pair(l, r, h, one);
         store_node(tree + 8 * (off + n + first / 2 + t), h);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) buf_a[j * (kMerkleBlockNodes / 2) + t] = h[j];
+        for (int j = 0; j < 8; ++j) buf_a[j * (kNarrowNodes / 2) + t] = h[j];
     }
     off += n;
     n >>= 1;
@@ -733,7 +753,7 @@ __global__ void __launch_bounds__(1024) k_merkle_block(uint32_t *__restrict__ tr
     m >>= 1;
     __syncthreads();
     uint32_t *src = buf_a, *dst = buf_b;
-    uint32_t ss = kMerkleBlockNodes / 2, ds = kMerkleBlockNodes / 4;
+    uint32_t ss = kNarrowNodes / 2, ds = kNarrowNodes / 4;
     while (m > 1) {
         if (t < m / 2) {
             uint32_t l[8], r[8], h[8];
@@ -762,25 +782,51 @@ __global__ void __launch_bounds__(1024) k_merkle_block(uint32_t *__restrict__ tr
     }
 }
 
+__global__ void __launch_bounds__(256) k_merkle_narrow(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
+                                                       uint32_t *ticket, uint32_t one) {
+    pdl_begin();
+    // layers in shared memory word-major (word j of node i at [j * stride +
+    // i]): a thread reads its two children's word j as one 8-byte load
+    __shared__ __align__(16) uint32_t buf_a[8 * (kNarrowNodes / 2)];
+    __shared__ __align__(16) uint32_t buf_b[8 * (kNarrowNodes / 4)];
+    __shared__ uint32_t last;
+    const uint32_t per = (uint32_t)(n_in < kNarrowNodes ? n_in : kNarrowNodes), nb = gridDim.x;
+    narrow_climb(tree, in_off, n_in, (uint64_t)blockIdx.x * per, per, buf_a, buf_b, one);
+    if (nb == 1) return;
+    // the layer of the blocks' roots
+    uint64_t off = in_off, n = n_in;
+    for (uint32_t m = per; m > 1; m >>= 1) { off += n; n >>= 1; }
+    __threadfence();  // this block's nodes are visible before its ticket
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == nb - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x == 0) *ticket = 0;  // ready for the next launch on the stream
+    narrow_climb(tree, off, n, 0, nb, buf_a, buf_b, one);
+}
+
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
-    if (num_leaves == 0 || (num_leaves & (num_leaves - 1))) return cudaErrorInvalidValue;
+    if (num_leaves == 0 || (num_leaves & (num_leaves - 1)) || !L.tickets) return cudaErrorInvalidValue;
     uint64_t off = 0, n = num_leaves;
     // Three layers per launch with a thread per 8 nodes while a layer has
-    // 2^18 nodes or more (every lane does full work); narrower layers go up
-    // eleven at a time in blocks of 2048 nodes, a layer per barrier.
+    // more than 2^18 nodes (every lane does full work); from a layer of
+    // 2^18 or fewer, one launch climbs to the root.
     while (n > 1) {
         cudaError_t e;
-        if (n >= (1ull << 18)) {
+        if (n > kNarrowMax) {
             const uint64_t threads = n / 8;
+            L.note(32.0 * (n + n / 2 + n / 4 + n / 8), (double)0, (double)(n / 2 + n / 4 + n / 8));
             LGK_LAUNCH(L, "merkle_thread3", launch_k(k_merkle_thread3, (unsigned)((threads + 127) / 128), 128, 0,
                                                      L.stream, tree, off, n, 1u));
             e = cudaGetLastError();
             for (int l = 0; l < 3; ++l) { off += n; n /= 2; }
         } else {
-            const uint64_t per = std::min<uint64_t>(n, kMerkleBlockNodes);
-            LGK_LAUNCH(L, "merkle_block", launch_k(k_merkle_block, (unsigned)(n / per), 1024, 0, L.stream, tree, off, n, 1u));
+            const uint64_t per = std::min<uint64_t>(n, kNarrowNodes);
+            L.note(32.0 * (2 * n - 1), 0, (double)(n - 1));
+            LGK_LAUNCH(L, "merkle_narrow", launch_k(k_merkle_narrow, (unsigned)(n / per), 256, 0, L.stream, tree, off,
+                                                    n, L.tickets, 1u));
             e = cudaGetLastError();
-            for (uint64_t m = per; m > 1; m /= 2) { off += n; n /= 2; }
+            n = 1;
         }
         if (e != cudaSuccess) return e;
     }
@@ -813,16 +859,12 @@ cudaError_t gather_opening(Launcher &L, const uint32_t *E, uint64_t rows, uint32
     const uint64_t total = (uint64_t)nq * ncols + 8ull * count;
     if (total == 0) return cudaSuccess;
     if (total > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    L.note(8.0 * total, 0);
     LGK_LAUNCH(L, "gather_opening", launch_k(k_gather_opening, (unsigned)((total + 255) / 256), 256, 0, L.stream, E,
                                              rows, ncols, d_queries, nq, tree, d_node_index, count, d_count, out));
     return cudaGetLastError();
 }
 
-// ================================================================= folds
-struct Coeffs64 { uint32_t v[64]; };
-
-// partial_eval over k top variables at once: out[i] = sum_j gr[j] in[j*M+i]
-// with gr the Lagrange (eq) basis of the k challenges; one table per gr[j].
 // evaluate_lagrange_basis (src/utils.rs:4-27) entry j of k challenges:
 // rs[0] selects the index MSB, factor rs[i] where the bit is set, 1 + rs[i]
 // where not (field products commute, so the order is immaterial).
@@ -832,50 +874,98 @@ __device__ __forceinline__ uint32_t lagrange_at(const uint32_t *rs, uint32_t k, 
     return p;
 }
 
-// NJ = 2^k values per output, loaded in runs of up to 8 independent loads
-// ahead of their products so that HBM latency overlaps.
-template <int NJ>
-__global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-                                                 uint64_t M, Coeffs64 gr, const uint32_t *d_rs, uint32_t k) {
+// ================================================================= folds
+// partial_eval over the top k variables (src/multilinear_poly.rs:66-87):
+// out[i] = the fold of in[j*M + i] over the k bits of j, each step
+// (1 + r) a + r b = a + r (a + b) on a pair (a, b) that differs in one bit of
+// j (b with the bit set).  The reference folds j's top bit first (with
+// rs[0]); folds of different variables commute and are exact, so folding
+// the lowest bit first (with rs[k-1]) gives the same field elements.  That
+// order lets a thread walk j upwards keeping one partial per level (a
+// binary counter: after leaf j, the trailing ones of j are the levels that
+// close), and all lanes of a warp multiply by the same challenge, so each
+// level needs one shared table.  A thread folds V consecutive outputs
+// (16-byte loads for V = 4), loads issued in runs of RUN leaves ahead of
+// their products.  2^k - 1 products per output.
+struct Rs6 { uint32_t v[6]; };
+
+template <int V>
+struct VecV { uint32_t x[V]; };
+
+template <int V>
+__device__ __forceinline__ VecV<V> load_v(const uint32_t *p) {
+    VecV<V> r;
+    if constexpr (V == 4) {
+        const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+        r.x[0] = t.x; r.x[1] = t.y; r.x[2] = t.z; r.x[3] = t.w;
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) r.x[v] = __ldg(p + v);
+    }
+    return r;
+}
+
+template <int K, int V>
+__global__ void __launch_bounds__(256) k_fold_tree(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                                                   uint64_t M, Rs6 rs, const uint32_t *d_rs) {
     pdl_begin();
-    extern __shared__ __align__(128) uint8_t tabs8[];
-    __shared__ uint32_t g[64];
+    __shared__ __align__(512) uint32_t tabs[K][kTabWords];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (threadIdx.x < NJ) g[threadIdx.x] = d_rs ? lagrange_at(d_rs, k, threadIdx.x) : gr.v[threadIdx.x];
+    for (int c = warp; c < K; c += nw) tab_build_warp(tabs[c], d_rs ? d_rs[c] : rs.v[c], lane);
     __syncthreads();
-    for (uint32_t j = warp; j < NJ; j += nw) tab_build_warp(reinterpret_cast<uint32_t *>(tabs8 + 512 * j), g[j], lane);
-    __syncthreads();
-    constexpr int RUN = NJ < 8 ? NJ : 8;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t acc = 0;
+    const uint8_t *t8 = reinterpret_cast<const uint8_t *>(&tabs[0][0]);
+    constexpr int NJ = 1 << K, RUN = NJ < 8 ? NJ : 8;
+    const uint64_t groups = M / V;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t *src = in + g * V;
+        VecV<V> st[K + 1];
 #pragma unroll
         for (int j0 = 0; j0 < NJ; j0 += RUN) {
-            uint32_t v[RUN];
+            VecV<V> leaf[RUN];
 #pragma unroll
-            for (int u = 0; u < RUN; ++u) v[u] = __ldg(in + (uint64_t)(j0 + u) * M + i);
+            for (int u = 0; u < RUN; ++u) leaf[u] = load_v<V>(src + (uint64_t)(j0 + u) * M);
 #pragma unroll
-            for (int u = 0; u < RUN; ++u) acc ^= tab_mul_sa(tabs8, 512u * (j0 + u), 0, v[u]);
+            for (int u = 0; u < RUN; ++u) {
+                const int j = j0 + u;
+                VecV<V> cur = leaf[u];
+                int c = 0;
+#pragma unroll
+                for (; c < K && ((j >> c) & 1); ++c) {
+                    // level c pairs j's bit c: left = st[c], right = cur,
+                    // challenge rs[K-1-c] (table K-1-c)
+#pragma unroll
+                    for (int v = 0; v < V; ++v)
+                        cur.x[v] = st[c].x[v] ^ tab_mul_sa(t8, 512u * (K - 1 - c), 0, st[c].x[v] ^ cur.x[v]);
+                }
+                st[c] = cur;
+            }
         }
-        out[i] = acc;
+        if constexpr (V == 4) {
+            *reinterpret_cast<uint4 *>(out + g * 4) = make_uint4(st[K].x[0], st[K].x[1], st[K].x[2], st[K].x[3]);
+        } else {
+#pragma unroll
+            for (int v = 0; v < V; ++v) out[g * V + v] = st[K].x[v];
+        }
     }
 }
 
 cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
-                    const uint32_t *gr, const uint32_t *d_rs) {
-    if (k < 1 || k > 6 || k > log_len || (!gr && !d_rs)) return cudaErrorInvalidValue;
-    Coeffs64 c{};
-    const uint32_t nj = 1u << k;
+                    const uint32_t *rs, const uint32_t *d_rs) {
+    if (k < 1 || k > 6 || k > log_len || (!rs && !d_rs)) return cudaErrorInvalidValue;
+    Rs6 c{};
     if (!d_rs)
-        for (uint32_t j = 0; j < nj; ++j) c.v[j] = gr[j];
+        for (uint32_t j = 0; j < k; ++j) c.v[j] = rs[j];
     const uint64_t M = 1ull << (log_len - k);
-    // four blocks per SM, each building its 2^k tables once for several
-    // runs of outputs (measured 10% faster than eight, 20% faster than two)
-    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((M + 255) / 256, 148ull * 4));
-    const size_t smem = nj * kTabWords * sizeof(uint32_t);
-    switch (nj) {
-#define LGK_CASE(n) \
-    case n: LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<n>, blocks, 256, smem, L.stream, in, out, M, c, d_rs, k)); break;
-        LGK_CASE(2) LGK_CASE(4) LGK_CASE(8) LGK_CASE(16) LGK_CASE(32) LGK_CASE(64)
+    const bool vec4 = M % 4 == 0 && ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
+    const uint64_t groups = vec4 ? M / 4 : M;
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * 8));
+    L.note(4.0 * (M << k) + 4.0 * M, (double)M * ((1u << k) - 1));
+    switch (k * 2 + (vec4 ? 1 : 0)) {
+#define LGK_CASE(kk)                                                                                              \
+    case 2 * kk: LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_tree<kk, 1>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); break; \
+    case 2 * kk + 1: LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_tree<kk, 4>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); break;
+        LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
     }
     return cudaGetLastError();
@@ -920,6 +1010,7 @@ cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t 
     const uint64_t half = 1ull << (log_len - 1);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((half + 255) / 256, 148ull * 4));
     const FsTail t = tail ? *tail : FsTail{};
+    L.note(16.0 * half, 3.0 * half);
     LGK_LAUNCH(L, "eval013", launch_k(k_eval013, blocks, 256, 0, L.stream, f, g, half, acc3, t));
     return cudaGetLastError();
 }
@@ -956,6 +1047,7 @@ cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32
     if (log_len < 2) return cudaErrorInvalidValue;
     const uint64_t quarter = 1ull << (log_len - 2);
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((quarter + 255) / 256, 148ull * 4));
+    L.note(48.0 * quarter, 7.0 * quarter);
     LGK_LAUNCH(L, "fold_round", launch_k(k_fold_round, blocks, 256, 0, L.stream, f, B, quarter, r, d_r, fo, Bo, acc3,
                                                                                 tail ? *tail : FsTail{}));
     return cudaGetLastError();
@@ -975,6 +1067,7 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
                  const uint32_t *d_beta) {
     const uint64_t n = 1ull << log_len;
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 4));
+    L.note(12.0 * n, (double)n);
     LGK_LAUNCH(L, "axpy", launch_k(k_axpy, blocks, 256, 0, L.stream, B, bi, n, beta, d_beta));
     return cudaGetLastError();
 }
@@ -1055,6 +1148,7 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
     if (!d_rs)
         for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
     for (uint32_t i = 0; i + 1 < n && i < 32; ++i) args.sks[i] = sks[i];
+    L.note(4.0 * nq * (glen + n + 2), (double)nq * (glen + 2 * n + 20));
     LGK_LAUNCH(L, "induce_setup", launch_k(k_induce_setup, (nq + 3) / 4, 128, 0, L.stream, d_rows, glen, d_q, nq,
                                            alpha, n, args, d_S, d_apow, d_rs, ilog2u(glen), d_alpha));
     return cudaGetLastError();
@@ -1152,12 +1246,15 @@ __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict_
 
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
                          uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum) {
+    const double vec = (double)nq * ((1ull << p.b) + (1ull << (n - p.b)));  // Lo and Hi words
+    L.note(4.0 * vec, vec);
     LGK_LAUNCH(L, "induce_prep",
                launch_k(k_induce_prep, nq, 256, 0, L.stream, d_S, d_apow, n, p.b, nq, d_lo, d_hi, d_sum));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 grid(1u << (n - p.b), p.qsplit);
     const int ao = p.qsplit > 1;
+    L.note(4.0 * (vec + (1ull << n)), (double)nq * (1ull << n));
     switch (std::max<uint32_t>(1, (1u << p.b) / 32)) {
 #define LGK_CASE(a) \
     case a: LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main<a>, grid, 256, 0, L.stream, d_lo, d_hi, n, p.b, nq, p.qsplit, out, ao)); break;
@@ -1338,6 +1435,7 @@ cudaError_t gf128_mul(Launcher &L, const uint64_t *a, const uint64_t *b, uint64_
     if (n == 0) return cudaSuccess;
     if ((uintptr_t)a % 16 || (uintptr_t)b % 16 || (uintptr_t)out % 16) return cudaErrorInvalidValue;
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 8);
+    L.note(48.0 * n, 0);
     LGK_LAUNCH(L, "gf128_mul", launch_k(k_gf128_mul, blocks, 256, 0, L.stream, reinterpret_cast<const ulonglong2 *>(a),
                                         reinterpret_cast<const ulonglong2 *>(b), reinterpret_cast<ulonglong2 *>(out), n));
     return cudaGetLastError();
@@ -1355,6 +1453,7 @@ __global__ void k_splitmix(uint64_t seed, uint32_t *out, uint64_t n) {
 }
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n) {
     const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 16));
+    L.note(4.0 * n, 0);
     LGK_LAUNCH(L, "splitmix", launch_k(k_splitmix, blocks, 256, 0, L.stream, seed, out, n));
     return cudaGetLastError();
 }

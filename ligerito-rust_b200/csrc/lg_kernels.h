@@ -27,6 +27,9 @@ struct Launcher {
     // stream order, each with the twiddle subtree it was built for and its
     // last use (the least recently used set is rebuilt first)
     uint32_t *dtab = nullptr;
+    // device words, owned by the context and zero between launches: block
+    // tickets of kernels whose last block to finish does the final step
+    uint32_t *tickets = nullptr;
     struct DtabKey {
         const uint32_t *tw = nullptr;
         uint32_t log_len = 0, root_base = 0;
@@ -39,6 +42,13 @@ struct Launcher {
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> free_events;
     std::map<std::string, std::pair<uint64_t, double>> stats;  // name -> (launches, ms)
+    // Algorithmic work of the timed launches, by kernel name: compulsory HBM
+    // bytes, GF(2^32) multiplications, BLAKE3 compressions.  A launcher
+    // states the next launch's work with note(); end() books it.
+    struct Work { double bytes = 0, mults = 0, comps = 0; };
+    std::map<std::string, Work> work;
+    Work next_work;
+    void note(double bytes, double mults, double comps = 0) { next_work = {bytes, mults, comps}; }
 
     cudaEvent_t get_event();
     void begin(const char *name, cudaEvent_t *a);
@@ -123,6 +133,7 @@ cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t 
 cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t b0,
                             uint32_t nb, uint32_t *out);
 // All upper layers from the leaf layer at tree[0]; tree as 8-word nodes.
+// Needs the Launcher's tickets.
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves);
 
 // --- gathers for openings (src/ligero.rs:40-51, src/merkle_tree.rs:98) ---
@@ -133,11 +144,11 @@ cudaError_t gather_opening(Launcher &L, const uint32_t *E, uint64_t rows, uint32
                            const uint32_t *d_count, uint32_t *out);
 
 // --- multilinear folds (src/multilinear_poly.rs:66-87) -------------------
-// out[i] = sum_j gr[j] * in[j*M + i], M = 2^log_len >> k, 1 <= k <= 6;
-// gr given on the host, or the Lagrange basis of the k device challenges
-// d_rs.
+// partial_eval of the top k variables (1 <= k <= 6): out (M = 2^log_len >> k
+// words) = sum_j eq(rs, j) * in[j*M + i], rs[0] for j's top bit; the k
+// challenges on the host (rs) or the device (d_rs).
 cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
-                    const uint32_t *gr, const uint32_t *d_rs = nullptr);
+                    const uint32_t *rs, const uint32_t *d_rs = nullptr);
 
 struct FsTail;  // a fused transcript step, below
 

@@ -9,8 +9,15 @@
 // entry point also needs scratch space (per-query subspace values, alpha
 // powers and the two expansion tables of the basis), which it takes from a
 // context that allocates.  Here that scratch is one fixed array in device
-// memory, reserved when the library is loaded and kept by every GPU that
-// loads the library until the process exits.
+// memory.  It sits in this file's own code module, which the CUDA runtime
+// loads lazily: the first call on a device loads the module, reserving the
+// array on that device (a driver allocation), and every GPU that has loaded
+// it keeps it until the process exits.  Callers make one warm-up call per
+// device at start-up; later calls allocate nothing.
+//
+// Queries are read as 32-bit row indices on the device (the regular entry
+// point rejects larger values on the host; here they stay on the device,
+// so values of 2^32 and more give undefined results).
 #include <cuda_runtime.h>
 
 #include <cstdint>

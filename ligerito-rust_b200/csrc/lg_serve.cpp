@@ -8,6 +8,11 @@
 // worker and memory free up, and their kernels and host transcript work
 // overlap with the others'.  A server with one worker is the FIFO loop of
 // the plain prover.
+//
+// Admission charges each request its peak device footprint, and the server
+// charges what its contexts keep between requests (arenas, FFT tables and
+// the device's shared code tables), so that the budget bounds the device
+// memory in use.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -18,6 +23,8 @@
 #include <thread>
 #include <unordered_map>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "../../include/ligerito_b200.h"
 #include "lg_host.h"
@@ -35,6 +42,9 @@ struct Request {
     std::vector<uint32_t> owned;  // copy of host input when asked for
     uint64_t mem = 0;             // admission footprint
     Clock::time_point t_submit, t_start, t_done;
+    int worker = -1;      // the worker that must prove it (-1: any)
+    int waiters = 0;      // threads inside lg_server_wait for it
+    bool claimed = false; // its result was handed out
     bool done = false;
     lg_status st = LG_OK;
     lg_proof *proof = nullptr;
@@ -65,19 +75,38 @@ struct lg_server {
     bool stop = false;
     Clock::time_point t0 = Clock::now();
 
-    void worker(lg_ctx *ctx) {
+    // device bytes the contexts keep between requests: each one's arena and
+    // FFT tables, and the code tables they share
+    uint64_t cached() const {
+        uint64_t b = lg_device_table_bytes(device);
+        for (auto *c : ctxs) b += lg_ctx_device_bytes_cached(c);
+        return b;
+    }
+
+    // the first queued request this worker may take (FIFO among those)
+    std::deque<Request *>::iterator next_for(int w) {
+        for (auto it = pending.begin(); it != pending.end(); ++it)
+            if ((*it)->worker < 0 || (*it)->worker == w) return it;
+        return pending.end();
+    }
+    bool admissible(const Request *r) const {
+        return budget == 0 || in_flight == 0 || r->mem + in_flight + cached() <= budget;
+    }
+
+    void worker(int w, lg_ctx *ctx) {
         for (;;) {
             Request *r = nullptr;
             {
                 std::unique_lock<std::mutex> lk(mu);
+                std::deque<Request *>::iterator it;
                 cv_work.wait(lk, [&] {
-                    return stop || (!pending.empty() && (budget == 0 || pending.front()->mem + in_flight <= budget ||
-                                                         in_flight == 0));
+                    if (stop && pending.empty()) return true;
+                    it = next_for(w);
+                    return it != pending.end() && admissible(*it);
                 });
                 if (stop && pending.empty()) return;
-                if (pending.empty()) continue;
-                r = pending.front();
-                pending.pop_front();
+                r = *it;
+                pending.erase(it);
                 in_flight += r->mem;
                 r->t_start = Clock::now();
             }
@@ -119,7 +148,10 @@ lg_status lg_server_create(int device, uint64_t hbm_budget_bytes, uint32_t worke
         }
         s->ctxs.push_back(c);
     }
-    for (auto *c : s->ctxs) s->threads.emplace_back([s, c] { s->worker(c); });
+    for (uint32_t i = 0; i < workers; ++i) {
+        lg_ctx *c = s->ctxs[i];
+        s->threads.emplace_back([s, i, c] { s->worker((int)i, c); });
+    }
     *out = s;
     return LG_OK;
 }
@@ -148,7 +180,7 @@ lg_status lg_server_submit(lg_server *s, const lg_config *cfg, const uint32_t *p
         s->pending.push_back(r.get());
         s->reqs.emplace(r->id, std::move(r));
     }
-    s->cv_work.notify_one();
+    s->cv_work.notify_all();
     return LG_OK;
 }
 
@@ -157,16 +189,31 @@ lg_status lg_server_wait(lg_server *s, uint64_t ticket, int64_t timeout_ms, lg_p
     if (!s || !proof) return LG_ERR_INVALID_ARGUMENT;
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->reqs.find(ticket);
-    if (it == s->reqs.end()) return LG_ERR_INVALID_ARGUMENT;
+    if (it == s->reqs.end() || it->second->claimed) return LG_ERR_INVALID_ARGUMENT;
     Request *r = it->second.get();
-    auto ready = [&] { return r->done; };
+    // the request stays in the map while any thread waits on it; the last
+    // one out after it was claimed erases it
+    ++r->waiters;
+    auto ready = [&] { return r->done || r->claimed; };
+    bool ok = true;
     if (timeout_ms < 0) s->cv_done.wait(lk, ready);
-    else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return LG_ERR_TIMEOUT;
-    *proof = r->proof;
-    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
-    if (queue_ms) *queue_ms = std::chrono::duration<double, std::milli>(r->t_start - r->t_submit).count();
-    lg_status st = r->st;
-    s->reqs.erase(it);
+    else ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready);
+    --r->waiters;
+    lg_status st;
+    if (r->claimed) {
+        st = LG_ERR_INVALID_ARGUMENT;  // another waiter took the result
+    } else if (!ok) {
+        return LG_ERR_TIMEOUT;
+    } else {
+        r->claimed = true;
+        *proof = r->proof;
+        r->proof = nullptr;
+        if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+        if (queue_ms) *queue_ms = std::chrono::duration<double, std::milli>(r->t_start - r->t_submit).count();
+        st = r->st;
+        s->cv_done.notify_all();  // other waiters on this ticket learn it was claimed
+    }
+    if (r->waiters == 0) s->reqs.erase(r->id);
     return st;
 }
 
@@ -191,6 +238,58 @@ void lg_server_destroy(lg_server *s) {
         if (kv.second->proof) lg_proof_free(kv.second->proof);
     for (auto *c : s->ctxs) lg_ctx_destroy(c);
     delete s;
+}
+
+lg_status lg_server_warm(lg_server *s, const lg_config *cfgs, uint32_t count) {
+    if (!s || (!cfgs && count)) return LG_ERR_INVALID_ARGUMENT;
+    uint64_t maxlen = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint64_t len = 1ull << (cfgs[i].initial_log_m + cfgs[i].initial_log_n);
+        if (lg::config_check(cfgs[i], len) != LG_OK) return LG_ERR_INVALID_CONFIG;
+        maxlen = std::max(maxlen, len);
+    }
+    if (!count) return LG_OK;
+    // one device input of the largest size; every warm-up proof reads a prefix
+    uint32_t *d = nullptr;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    if (cudaMalloc(&d, 4 * maxlen) != cudaSuccess) {
+        cudaGetLastError();
+        cudaSetDevice(prev);
+        return LG_ERR_OUT_OF_MEMORY;
+    }
+    lg_status st = lg_fill_splitmix(s->ctxs[0], 0, d, maxlen);
+    if (st == LG_OK) st = lg_ctx_synchronize(s->ctxs[0]);
+    std::vector<uint64_t> tickets;
+    if (st == LG_OK) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (uint32_t i = 0; i < count; ++i)
+            for (size_t w = 0; w < s->ctxs.size(); ++w) {
+                auto r = std::make_unique<Request>();
+                r->cfg = cfgs[i];
+                r->len = 1ull << (cfgs[i].initial_log_m + cfgs[i].initial_log_n);
+                r->poly = d;
+                r->on_device = 1;
+                r->worker = (int)w;
+                r->mem = 0;  // warm-up runs outside the budget
+                r->t_submit = Clock::now();
+                r->id = s->next_id++;
+                tickets.push_back(r->id);
+                s->pending.push_back(r.get());
+                s->reqs.emplace(r->id, std::move(r));
+            }
+    }
+    s->cv_work.notify_all();
+    for (uint64_t t : tickets) {
+        lg_proof *p = nullptr;
+        lg_status x = lg_server_wait(s, t, -1, &p, nullptr, nullptr);
+        if (p) lg_proof_free(p);
+        if (x != LG_OK && st == LG_OK) st = x;
+    }
+    cudaFree(d);
+    cudaSetDevice(prev);
+    return st;
 }
 
 lg_status lg_prove_batch(int device, uint32_t workers, const lg_config *cfgs, const uint32_t *const *polys,

@@ -8,6 +8,7 @@ ROOT = pathlib.Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "oracle"))
 GOLDEN = ROOT / "tests" / "golden" / "golden.json"
+GOLDEN_LARGE = ROOT / "tests" / "golden" / "golden_large.json"
 
 
 def pytest_configure(config):
@@ -33,6 +34,11 @@ def lg():
 @pytest.fixture(scope="session")
 def golden():
     return json.loads(GOLDEN.read_text())
+
+
+@pytest.fixture(scope="session")
+def golden_large():
+    return json.loads(GOLDEN_LARGE.read_text())
 
 
 @pytest.fixture(scope="session")

@@ -40,7 +40,7 @@ def test_fft_zero_and_constant_vectors(lg, ref, ctx):
 
 
 @pytest.mark.parametrize("log_n,batch", [(16, 1024), (20, 64), (22, 16)])
-def test_fft_microbench_sizes_roundtrip(lg, ref, ctx, log_n, batch):
+def test_fft_microbench_sizes_roundtrip(lg, ref, ctx, golden_large, log_n, batch):
     # the 256 MiB batched transforms of the fft/ifft microbench: ifft(fft(v))
     # == v everywhere, one vector checked against the oracle, and the
     # transform is linear (fft(a ^ b) == fft(a) ^ fft(b)) on a sample
@@ -52,6 +52,12 @@ def test_fft_microbench_sizes_roundtrip(lg, ref, ctx, log_n, batch):
     if log_n <= 20:
         col = lg.to_host(keep[:1 << log_n])
         assert (lg.to_host(d[:1 << log_n]) == ref.fft(col)).all()
+    else:  # the oracle's transform of the first vector, committed as a digest
+        k = golden_large["kernels"]
+        assert hashlib.sha256(lg.to_host(d[:1 << log_n]).tobytes()).hexdigest() == k["fft22_seed1_first_sha256"]
+        first = keep[:1 << log_n].clone()
+        lg.ifft(first, log_n, ctx)
+        assert hashlib.sha256(lg.to_host(first).tobytes()).hexdigest() == k["ifft22_seed1_first_sha256"]
     a, b = keep[: 2 << log_n].clone(), lg.splitmix_coeffs_device(9, 2 << log_n, ctx)
     ab = torch.bitwise_xor(a, b)
     for t in (a, b, ab):

@@ -99,7 +99,10 @@ def test_config24_matches_oracle(lg, ref, ctx):
 
 
 @pytest.mark.parametrize("L", [17, 18, 19, 21, 22])
-def test_generated_configs_verify(lg, ref, ctx, L):
+def test_generated_configs_match_oracle(lg, ref, ctx, golden_large, L):
+    # generated configs (the config.rs pattern extended): byte-identical to
+    # the oracle's proof -- re-proved here up to 2^19, against the oracle's
+    # committed digest (tests/golden/make_golden_large.py) above
     cfg = lg.config_for_size(L)
     poly = lg.splitmix_coeffs_device(L, cfg.poly_len, ctx)
     proof = lg.prover(cfg, poly, ctx)
@@ -108,6 +111,38 @@ def test_generated_configs_verify(lg, ref, ctx, L):
     assert ref.verify(ref.config_make(L), b, nthreads=8) == (ref.OK, True)
     if L <= 19:
         assert b == ref.prove(ref.config_make(L), lg.to_host(poly), nthreads=8)
+    else:
+        case = golden_large["cases"][f"cfg{L}_seed{L}"]
+        assert len(b) == case["proof_len"]
+        assert hashlib.sha256(b).hexdigest() == case["proof_sha256"]
+        f = proof.fields()
+        assert [f.initial_root.hex()] + [r.hex() for r in f.recursive_roots] == case["roots"]
+
+
+def test_config24_matches_golden_digest(lg, ctx, golden_large):
+    cfg = lg.hardcoded_config_24()
+    b = lg.prover(cfg, lg.splitmix_coeffs_device(1, 1 << 24, ctx), ctx).to_bytes()
+    assert hashlib.sha256(b).hexdigest() == golden_large["cases"]["cfg24_seed1"]["proof_sha256"]
+
+
+def test_config28_matches_oracle_digest(lg, ref, ctx, golden_large):
+    # 2^28 coefficients (1 GiB input, 4 GiB first encoded matrix, seed 2,
+    # the generated config): byte-identical to the oracle's proof (its
+    # digest, roots and challenges, committed), accepted by both verifiers
+    import os
+
+    case = golden_large["cases"]["cfg28_seed2"]
+    cfg = lg.config_for_size(28)
+    poly = lg.splitmix_coeffs_device(2, cfg.poly_len, ctx)
+    proof = lg.prover(cfg, poly, ctx)
+    del poly
+    b = proof.to_bytes()
+    f = proof.fields()
+    assert [f.initial_root.hex()] + [r.hex() for r in f.recursive_roots] == case["roots"]
+    assert len(b) == case["proof_len"]
+    assert hashlib.sha256(b).hexdigest() == case["proof_sha256"]
+    assert lg.verifier(cfg, proof, ctx)
+    assert ref.verify(ref.config_make(28), b, nthreads=os.cpu_count() or 8) == (ref.OK, True)
 
 
 def test_proving_is_deterministic(lg, ctx):

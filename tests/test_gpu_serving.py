@@ -31,7 +31,9 @@ def test_server_mixed_stream_with_budget(lg, ctx):
     sizes = [16, 20, 17, 18, 20, 16, 19, 16, 20, 18, 17, 16, 19, 20, 16, 18]
     seeds = [4 + i for i in range(len(sizes))]
     want = _alone(lg, ctx, sizes, seeds)
-    srv = lg.Server(0, workers=4, hbm_budget_bytes=2 * (24 << 20) + 2 * (48 << 20))
+    # admission charges the contexts' own arenas and tables as well
+    cached = 4 * lg.lib.lg_ctx_device_bytes_cached(ctx.handle) + (64 << 20)
+    srv = lg.Server(0, workers=4, hbm_budget_bytes=cached + 2 * (28 << 20) + 2 * (48 << 20))
     try:
         tickets = []
         for L, s in zip(sizes, seeds):
@@ -78,5 +80,49 @@ def test_single_worker_server_is_fifo(lg, ctx):
         # with one worker each request waits for everything submitted before it
         lats = [r[1] for r in results]
         assert lats[0] <= lats[1] <= lats[2]
+    finally:
+        srv.close()
+
+
+def test_two_waiters_on_one_ticket_get_one_result(lg, ctx):
+    # the result is handed out once; the other waiter is told the ticket is
+    # gone instead of reading a freed request
+    import threading
+
+    srv = lg.Server(0, workers=1)
+    try:
+        cfg = lg.config_for_size(20)
+        t = srv.submit(cfg, lg.splitmix_coeffs_device(20, cfg.poly_len, ctx))
+        out = []
+
+        def waiter():
+            try:
+                out.append(("proof", srv.wait(t)[0].to_bytes()))
+            except lg.LigeritoError as e:
+                out.append(("error", e.status))
+
+        ths = [threading.Thread(target=waiter) for _ in range(3)]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        assert sorted(k for k, _ in out) == ["error", "error", "proof"]
+        assert all(v == 1 for k, v in out if k == "error")
+        with pytest.raises(lg.LigeritoError) as e:
+            srv.wait(t)
+        assert e.value.status == 1
+    finally:
+        srv.close()
+
+
+def test_server_warm_then_same_bytes(lg, ctx):
+    srv = lg.Server(0, workers=3)
+    try:
+        cfgs = [lg.config_for_size(L) for L in (16, 18)]
+        srv.warm(cfgs)
+        assert srv.stats()["completed"] == 6
+        want = _alone(lg, ctx, [18], [77])[0]
+        t = srv.submit(cfgs[1], lg.splitmix_coeffs_device(77, cfgs[1].poly_len, ctx))
+        assert srv.wait(t)[0].to_bytes() == want
     finally:
         srv.close()

@@ -55,6 +55,35 @@ def test_noalloc_matches_regular_entry_point_twice(lg, ctx):
         assert int(sum_d.cpu().numpy().view(np.uint32)[0]) == want_sum
 
 
+def test_noalloc_on_a_caller_stream_runs_after_the_callers_work(lg, ctx):
+    # Work queued on the caller's stream runs behind what the caller queued
+    # there before: a write of garbage into the outputs, queued just ahead
+    # of the call on the same stream, must be overwritten by the result.
+    import torch
+
+    rng = np.random.default_rng(99)
+    n, nch = 14, 6
+    rows, q, ch, alpha = _inputs(rng, n, nch)
+    want_basis, want_sum = lg.induce_sumcheck_poly(n, rows, ch, q, alpha, ctx)
+    rows_d = torch.from_numpy(rows.reshape(-1).view(np.int32)).cuda()
+    q_d = torch.from_numpy(q.view(np.int64)).cuda()
+    out_d = torch.zeros((1 << n,), dtype=torch.int32, device="cuda")
+    sum_d = torch.zeros((1,), dtype=torch.int32, device="cuda")
+    ch = np.ascontiguousarray(ch, dtype=np.uint32)
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        torch.cuda._sleep(1 << 20)  # keeps the stream busy while the call is queued
+        out_d.fill_(0x33333333)
+        sum_d.fill_(0x33333333)
+    st = lg.lib.lg_induce_sumcheck_poly_noalloc(s.cuda_stream, n, rows_d.data_ptr(), rows.shape[0], ch.ctypes.data,
+                                                 ch.size, q_d.data_ptr(), alpha, out_d.data_ptr(), sum_d.data_ptr())
+    assert st == 0
+    s.synchronize()
+    assert torch.equal(out_d, want_basis)
+    assert int(sum_d.cpu().numpy().view(np.uint32)[0]) == want_sum
+
+
 def test_noalloc_refuses_sizes_past_its_scratch(lg):
     import torch
 
