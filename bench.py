@@ -325,6 +325,12 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
         }
+        if world == 1 and not args.no_mixed:
+            # the mixed-size forms against the plain GPU prover: 64 uneven
+            # proofs batched vs looped, and a served Poisson stream vs a FIFO
+            # loop at matched p99 (10,000 requests per offered rate)
+            line["batch64"] = batch64(lg, 3, 1)
+            line["serve"] = serve_sweep(lg, 10000, [1000, 2000, 4000, 8000], 8)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -486,7 +492,7 @@ def _pct(xs, q):
     return xs[min(len(xs) - 1, int(round(q * (len(xs) - 1))))] if xs else None
 
 
-def run_batch64(args):
+def batch64(lg, steps: int, warmup: int, workers=(4, 8)) -> dict:
     """64 polynomials, log sizes uniform in {16..22} (seed 3), poly i from
     SplitMix64 seed 3*2^32 + i, device-resident: a loop of the plain prover
     on one context vs the server's concurrent workers.  Wall-clock makespan
@@ -494,10 +500,6 @@ def run_batch64(args):
     import numpy as np
     import torch
 
-    sys.path.insert(0, str(ROOT))
-    import __graft_entry__ as g
-
-    lg = g.load_package()
     ctx = lg.Context(0)
     rng = np.random.default_rng(3)
     sizes = [int(x) for x in rng.integers(16, 23, size=64)]
@@ -522,17 +524,18 @@ def run_batch64(args):
             done.append(time.perf_counter() - t0)
         return max(done), done
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         loop()
-    res = {}
-    tl = [loop() for _ in range(args.steps)]
-    res["loop"] = tl
-    for w in (4, 8):
+    res = {"loop": [loop() for _ in range(steps)]}
+    uniq = [lg.config_for_size(L) for L in sorted(set(sizes))]
+    for w in workers:
         srv = lg.Server(0, workers=w)
-        for _ in range(max(1, args.warmup)):
+        srv.warm(uniq)
+        for _ in range(max(1, warmup)):
             batched(srv)
-        res[f"workers{w}"] = [batched(srv) for _ in range(args.steps)]
+        res[f"workers{w}"] = [batched(srv) for _ in range(steps)]
         srv.close()
+    ctx.close()
     out = {}
     for k, runs in res.items():
         mk = statistics.median(r[0] for r in runs)
@@ -540,43 +543,44 @@ def run_batch64(args):
         out[k] = {"proofs_per_s": round(64 / mk, 1), "makespan_ms": round(mk * 1e3, 2),
                   "p50_ms": round(_pct(comp, 0.5), 2), "p99_ms": round(_pct(comp, 0.99), 2)}
     best = max((k for k in out if k != "loop"), key=lambda k: out[k]["proofs_per_s"])
-    print(json.dumps({"workload": "batch64", "metric": "mixed-size proofs/s, batched vs plain GPU loop",
-                      "value": out[best]["proofs_per_s"], "unit": "proofs/s", "higher_is_better": True,
-                      "speedup_vs_loop": round(out[best]["proofs_per_s"] / out["loop"]["proofs_per_s"], 2),
-                      "steps": args.steps, "warmup": args.warmup, "sizes_log2": sizes,
-                      "data": "synthetic (SplitMix64), device-resident", "results": out}), flush=True)
+    return {"workload": "batch64", "metric": "mixed-size proofs/s, batched vs plain GPU loop",
+            "value": out[best]["proofs_per_s"], "unit": "proofs/s", "higher_is_better": True, "best": best,
+            "speedup_vs_loop": round(out[best]["proofs_per_s"] / out["loop"]["proofs_per_s"], 2),
+            "steps": steps, "warmup": warmup, "sizes_log2": sizes,
+            "data": "synthetic (SplitMix64), device-resident", "results": out}
 
 
-def run_serve(args):
+def run_batch64(args):
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as g
+
+    print(json.dumps(batch64(g.load_package(), args.steps, args.warmup)), flush=True)
+
+
+def serve_sweep(lg, n_req: int, rates, workers: int, log=None) -> dict:
     """Poisson arrivals of proof requests, log sizes in {16..24} with
     P(s) ~ 2^(-(s-16)/2), coefficients SplitMix64 seed 4+i generated on the
     device as each request arrives, 160 GB admission budget.  The FIFO loop
     of the plain prover is the same server with one worker on the same
-    arrival trace."""
+    arrival trace.  Both arms are compared at matched p99: the FIFO arm's
+    operating point is the highest offered rate it keeps up with (at least
+    95% of the offered rate completed per second), and the served arm's is
+    the highest throughput whose p99 is no higher than that point's."""
     import threading
 
     import numpy as np
-    import torch
 
-    sys.path.insert(0, str(ROOT))
-    import __graft_entry__ as g
-
-    lg = g.load_package()
     gen = lg.Context(0)
-    n_req = args.requests
     rng = np.random.default_rng(5)
     svals = np.arange(16, 25)
     pw = 2.0 ** (-(svals - 16) / 2.0)
     sizes = rng.choice(svals, size=n_req, p=pw / pw.sum())
     cfg_by = {int(L): lg.config_for_size(int(L)) for L in svals}
     budget = 160 * 10**9
-    rates = [float(r) for r in args.rates.split(",")]
     results = []
-    for workers in (1, args.workers):
-        srv = lg.Server(0, workers=workers, hbm_budget_bytes=budget)
-        for L in svals:  # warm every worker's tables for every size
-            for _ in range(workers):
-                srv.wait(srv.submit(cfg_by[int(L)], lg.splitmix_coeffs_device(0, cfg_by[int(L)].poly_len, gen)))
+    for nw in (1, workers):
+        srv = lg.Server(0, workers=nw, hbm_budget_bytes=budget)
+        srv.warm([cfg_by[int(L)] for L in svals])
         for rate in rates:
             gaps = np.random.default_rng(int(rate)).exponential(1.0 / rate, size=n_req)
             lat, keep, tickets = [], {}, []
@@ -610,23 +614,33 @@ def run_serve(args):
                     tickets.append(t)
             th.join()
             span = time.perf_counter() - t0
-            results.append({"workers": workers, "offered_per_s": rate, "proofs_per_s": round(n_req / span, 1),
+            results.append({"workers": nw, "offered_per_s": rate, "proofs_per_s": round(n_req / span, 1),
                             "p50_ms": round(_pct(lat, 0.5), 3), "p99_ms": round(_pct(lat, 0.99), 3)})
-            print(json.dumps(results[-1]), file=sys.stderr, flush=True)
+            if log:
+                print(json.dumps(results[-1]), file=log, flush=True)
         srv.close()
+    gen.close()
     fifo = [r for r in results if r["workers"] == 1]
     served = [r for r in results if r["workers"] != 1]
-    # highest rate each arm sustains with p99 within 4x its lightest-load p99
-    def sustained(rs):
-        ok = [r for r in rs if r["p99_ms"] <= 4 * rs[0]["p99_ms"]]
-        return max(ok, key=lambda r: r["proofs_per_s"]) if ok else rs[0]
-    f, s_ = sustained(fifo), sustained(served)
-    print(json.dumps({"workload": "serve", "metric": "served proofs/s at saturation-bounded p99 vs FIFO plain loop",
-                      "value": s_["proofs_per_s"], "unit": "proofs/s", "higher_is_better": True,
-                      "speedup_vs_fifo": round(s_["proofs_per_s"] / f["proofs_per_s"], 2),
-                      "p99_ms": s_["p99_ms"], "fifo": f, "requests": n_req, "workers": args.workers,
-                      "data": "synthetic (SplitMix64 seed 4+i, generated on device at arrival)",
-                      "sweep": results}), flush=True)
+    kept = [r for r in fifo if r["proofs_per_s"] >= 0.95 * r["offered_per_s"]] or fifo[:1]
+    f = max(kept, key=lambda r: r["proofs_per_s"])
+    ok = [r for r in served if r["p99_ms"] <= f["p99_ms"]]
+    s_ = max(ok, key=lambda r: r["proofs_per_s"]) if ok else None
+    return {"workload": "serve", "metric": "served proofs/s at a p99 no higher than the FIFO plain loop's",
+            "value": s_["proofs_per_s"] if s_ else None, "unit": "proofs/s", "higher_is_better": True,
+            "speedup_vs_fifo": round(s_["proofs_per_s"] / f["proofs_per_s"], 2) if s_ else None,
+            "p99_ms": s_["p99_ms"] if s_ else None, "fifo": f, "served": s_, "requests": n_req,
+            "workers": workers, "data": "synthetic (SplitMix64 seed 4+i, generated on device at arrival)",
+            "sweep": results}
+
+
+def run_serve(args):
+    sys.path.insert(0, str(ROOT))
+    import __graft_entry__ as g
+
+    rates = [float(r) for r in args.rates.split(",")]
+    print(json.dumps(serve_sweep(g.load_package(), args.requests, rates, args.workers, log=sys.stderr)),
+          flush=True)
 
 
 def main():
@@ -639,8 +653,9 @@ def main():
                     choices=["prove24", "prove28", "commit24", "fft16", "fft20", "fft22", "ifft16", "ifft20", "ifft22",
                              "batch64", "serve", "verify24"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests per rate")
-    ap.add_argument("--rates", default="500,1000,2000,4000,8000,16000", help="serve: offered rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=10000, help="serve: number of requests per rate")
+    ap.add_argument("--rates", default="1000,2000,3000,4000,6000,8000", help="serve: offered rates (requests/s)")
+    ap.add_argument("--no-mixed", action="store_true", help="prove24: skip the batch64 / serve objects")
     ap.add_argument("--workers", type=int, default=8, help="serve: concurrent workers")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -145,6 +145,11 @@ lg_status lg_prove(lg_ctx *ctx, const lg_config *cfg, const uint32_t *poly, uint
  * *accepted = the reference's return value; LG_ERR_VERIFY_PANIC (accepted =
  * 0) where the reference panics (Merkle / Ligero asserts, malformed sizes). */
 lg_status lg_verify(lg_ctx *ctx, const lg_config *cfg, const lg_proof *proof, int *accepted);
+/* The same from the proof's bytes (lg_proof_serialize's encoding), so a
+ * caller holding only bytes needs no parser: LG_ERR_MALFORMED_PROOF when
+ * they do not parse, otherwise as lg_verify (verifier.rs:10). */
+lg_status lg_verify_bytes(lg_ctx *ctx, const lg_config *cfg, const uint8_t *proof, uint64_t len,
+                          int *accepted);
 
 /* Canonical byte encoding in the field order of FinalizedLigeritoProof
  * (src/data_structures.rs:91-103); the reference keeps proofs in memory

@@ -107,6 +107,7 @@ def _load() -> ctypes.CDLL:
         "lg_server_warm": (i32, [P, P, u32]),
         "lg_prove": (i32, [P, P, P, u64, i32, P]),
         "lg_verify": (i32, [P, P, P, P]),
+        "lg_verify_bytes": (i32, [P, P, ctypes.c_char_p, u64, P]),
         "lg_proof_serialize": (i32, [P, P, P]),
         "lg_proof_deserialize": (i32, [P, u64, P]),
         "lg_proof_free": (None, [P]),
@@ -585,9 +586,11 @@ def verifier(config, proof, ctx: Optional[Context] = None) -> bool:
     if isinstance(config, ProverConfig):
         config = _to_verifier(config)
     c = config.to_c()
-    if isinstance(proof, (bytes, bytearray)):
-        proof = FinalizedLigeritoProof.from_bytes(bytes(proof))
     acc = ctypes.c_int()
+    if isinstance(proof, (bytes, bytearray)):
+        b = bytes(proof)
+        _check(lib.lg_verify_bytes(ctx.handle, ctypes.byref(c), b, len(b), ctypes.byref(acc)), ctx)
+        return bool(acc.value)
     _check(lib.lg_verify(ctx.handle, ctypes.byref(c), proof.handle, ctypes.byref(acc)), ctx)
     return bool(acc.value)
 

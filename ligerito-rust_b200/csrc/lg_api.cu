@@ -1378,6 +1378,13 @@ lg_status lg_proof_serialize(const lg_proof *p, uint8_t *buf, uint64_t *len) {
     return LG_OK;
 }
 
+lg_status lg_verify_bytes(lg_ctx *c, const lg_config *cfg, const uint8_t *proof, uint64_t len, int *accepted) {
+    if (!c || !cfg || !proof || !accepted) return LG_ERR_INVALID_ARGUMENT;
+    *accepted = 0;
+    lg_proof p;
+    if (!lg::deserialize(proof, len, p.p)) return LG_ERR_MALFORMED_PROOF;
+    return lg_verify(c, cfg, &p, accepted);
+}
 lg_status lg_proof_deserialize(const uint8_t *buf, uint64_t len, lg_proof **out) {
     if (!buf || !out) return LG_ERR_INVALID_ARGUMENT;
     *out = nullptr;

@@ -100,37 +100,61 @@ __global__ void k_rs_scale(const uint32_t *__restrict__ poly, const uint32_t *__
 }
 
 // The same scaling for many columns: every column multiplies row i by the
-// same pis[i], so a block takes 32 rows x up to 64 columns, builds the 32
-// rows' multiplication tables and multiplies with table lookups that every
-// lane of a warp shares.  The tile goes through shared memory with an odd
-// column stride: rows along lanes for the coalesced global accesses,
-// columns along lanes for the lookups, both free of bank conflicts.
-constexpr uint32_t kScaleRows = 32, kScaleCols = 64;
-__global__ void __launch_bounds__(256) k_rs_scale_tab(const uint32_t *__restrict__ poly,
-                                                      const uint32_t *__restrict__ pis, uint32_t *__restrict__ out,
-                                                      uint32_t log_m, uint32_t n) {
+// same pis[i], so a block takes tiles of 32 rows x up to 64 columns, builds
+// the 32 rows' multiplication tables and multiplies with table lookups that
+// every lane of a warp shares.  A tile goes through shared memory with an
+// odd column stride: rows along lanes for the coalesced global accesses,
+// columns along lanes for the lookups, both free of bank conflicts.  Blocks
+// loop over tiles and load the next tile into registers before multiplying
+// the current one, so its HBM latency hides behind the table builds and
+// lookups.
+constexpr uint32_t kScaleRows = 32, kScaleCols = 64, kScaleThreads = 256;
+constexpr uint32_t kScalePer = kScaleRows * kScaleCols / kScaleThreads;  // words per thread
+__global__ void __launch_bounds__(kScaleThreads) k_rs_scale_tab(const uint32_t *__restrict__ poly,
+                                                                const uint32_t *__restrict__ pis,
+                                                                uint32_t *__restrict__ out, uint32_t log_m, uint32_t n) {
     pdl_begin();
     __shared__ __align__(512) uint32_t tabs[kScaleRows][kTabWords];
     __shared__ uint32_t tile[kScaleCols * (kScaleRows + 1)];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t m = 1ull << log_m;
-    const uint64_t i0 = (uint64_t)blockIdx.x * kScaleRows;
+    const uint32_t ntiles = (uint32_t)(m / kScaleRows);
     const uint32_t j0 = blockIdx.y * kScaleCols, ncol = min(kScaleCols, n - j0);
-    for (uint32_t r = warp; r < kScaleRows; r += blockDim.x >> 5) tab_build_warp(tabs[r], __ldg(pis + i0 + r), lane);
-    for (uint32_t c = threadIdx.x; c < ncol * kScaleRows; c += blockDim.x) {
-        const uint32_t j = c / kScaleRows, r = c % kScaleRows;
-        tile[j * (kScaleRows + 1) + r] = __ldg(poly + (uint64_t)(j0 + j) * m + i0 + r);
-    }
-    __syncthreads();
-    for (uint32_t r = warp; r < kScaleRows; r += blockDim.x >> 5)
-        for (uint32_t j = lane; j < ncol; j += 32) {
-            uint32_t *x = tile + j * (kScaleRows + 1) + r;
-            *x = tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * r, 0, *x);
+    // thread's slots c = threadIdx.x + 256 i: column c / 32, row c % 32
+    uint32_t pre[kScalePer];
+    auto load = [&](uint32_t t) {
+        const uint64_t i0 = (uint64_t)t * kScaleRows;
+#pragma unroll
+        for (uint32_t i = 0; i < kScalePer; ++i) {
+            const uint32_t c = threadIdx.x + kScaleThreads * i, j = c / kScaleRows, r = c % kScaleRows;
+            pre[i] = j < ncol ? __ldg(poly + (uint64_t)(j0 + j) * m + i0 + r) : 0u;
         }
-    __syncthreads();
-    for (uint32_t c = threadIdx.x; c < ncol * kScaleRows; c += blockDim.x) {
-        const uint32_t j = c / kScaleRows, r = c % kScaleRows;
-        out[(uint64_t)(j0 + j) * m + i0 + r] = tile[j * (kScaleRows + 1) + r];
+    };
+    uint32_t t = blockIdx.x;
+    if (t < ntiles) load(t);
+    for (; t < ntiles; t += gridDim.x) {
+        const uint64_t i0 = (uint64_t)t * kScaleRows;
+        for (uint32_t r = warp; r < kScaleRows; r += kScaleThreads / 32)
+            tab_build_warp(tabs[r], __ldg(pis + i0 + r), lane);
+#pragma unroll
+        for (uint32_t i = 0; i < kScalePer; ++i) {
+            const uint32_t c = threadIdx.x + kScaleThreads * i;
+            tile[(c / kScaleRows) * (kScaleRows + 1) + c % kScaleRows] = pre[i];
+        }
+        __syncthreads();
+        if (t + gridDim.x < ntiles) load(t + gridDim.x);  // in flight during the lookups
+        for (uint32_t r = warp; r < kScaleRows; r += kScaleThreads / 32)
+            for (uint32_t j = lane; j < ncol; j += 32) {
+                uint32_t *x = tile + j * (kScaleRows + 1) + r;
+                *x = tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * r, 0, *x);
+            }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t i = 0; i < kScalePer; ++i) {
+            const uint32_t c = threadIdx.x + kScaleThreads * i, j = c / kScaleRows, r = c % kScaleRows;
+            if (j < ncol) out[(uint64_t)(j0 + j) * m + i0 + r] = tile[j * (kScaleRows + 1) + r];
+        }
+        __syncthreads();  // the tile and tables are rewritten next
     }
 }
 
@@ -139,7 +163,9 @@ cudaError_t rs_scale(Launcher &L, const uint32_t *poly, const uint32_t *pis, uin
     if (n >= kScaleCols / 2 && log_m >= 5) {
         // a table costs about as much as 30 general products: worth it from
         // 32 columns on
-        const dim3 grid((unsigned)((1ull << log_m) / kScaleRows), (n + kScaleCols - 1) / kScaleCols);
+        // a few tiles per block: about four blocks per SM in one wave
+        const uint64_t ntiles = (1ull << log_m) / kScaleRows;
+        const dim3 grid((unsigned)std::min<uint64_t>(ntiles, 148ull * 4), (n + kScaleCols - 1) / kScaleCols);
         L.note(8.0 * n * (1ull << log_m), (double)n * (1ull << log_m));
         LGK_LAUNCH(L, "rs_scale", launch_k(k_rs_scale_tab, grid, 256, 0, L.stream, poly, pis, out, log_m, n));
         return cudaGetLastError();
@@ -876,77 +902,52 @@ __device__ __forceinline__ uint32_t lagrange_at(const uint32_t *rs, uint32_t k, 
 
 // ================================================================= folds
 // partial_eval over the top k variables (src/multilinear_poly.rs:66-87):
-// out[i] = the fold of in[j*M + i] over the k bits of j, each step
-// (1 + r) a + r b = a + r (a + b) on a pair (a, b) that differs in one bit of
-// j (b with the bit set).  The reference folds j's top bit first (with
-// rs[0]); folds of different variables commute and are exact, so folding
-// the lowest bit first (with rs[k-1]) gives the same field elements.  That
-// order lets a thread walk j upwards keeping one partial per level (a
-// binary counter: after leaf j, the trailing ones of j are the levels that
-// close), and all lanes of a warp multiply by the same challenge, so each
-// level needs one shared table.  A thread folds V consecutive outputs
-// (16-byte loads for V = 4), loads issued in runs of RUN leaves ahead of
-// their products.  2^k - 1 products per output.
+// out[i] = sum_j eq(rs, j) in[j*M + i], j's top bit with rs[0] -- the
+// reference's sequence of folds (1 + r) a + r b, each exact, collapsed into
+// one sum of products (the same field element).  The eq weights split over
+// j = (jh, jl): eq(rs, j) = eq(rs[..kh], jh) * eq(rs[kh..], jl), so
+// out[i] = sum_jh EH[jh] * (sum_jl EL[jl] * in[(jh 2^kl + jl) M + i]): the
+// inner sums take 2^k products over 2^kl tables shared by every lane, the
+// outer 2^kh more over 2^kh tables.  A block builds its 2^kl + 2^kh tables
+// once and then loops over outputs; every product in an inner sum is
+// independent of the others, so loads and lookups overlap.
 struct Rs6 { uint32_t v[6]; };
 
-template <int V>
-struct VecV { uint32_t x[V]; };
-
-template <int V>
-__device__ __forceinline__ VecV<V> load_v(const uint32_t *p) {
-    VecV<V> r;
-    if constexpr (V == 4) {
-        const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
-        r.x[0] = t.x; r.x[1] = t.y; r.x[2] = t.z; r.x[3] = t.w;
-    } else {
-#pragma unroll
-        for (int v = 0; v < V; ++v) r.x[v] = __ldg(p + v);
-    }
-    return r;
-}
-
-template <int K, int V>
-__global__ void __launch_bounds__(256) k_fold_tree(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-                                                   uint64_t M, Rs6 rs, const uint32_t *d_rs) {
+template <int KH, int KL>
+__global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                                                 uint64_t M, Rs6 rs, const uint32_t *d_rs) {
     pdl_begin();
-    __shared__ __align__(512) uint32_t tabs[K][kTabWords];
+    constexpr int NH = 1 << KH, NL = 1 << KL;
+    __shared__ __align__(512) uint32_t tabs[NH + NL][kTabWords];  // EL tables, then EH
+    __shared__ uint32_t r[KH + KL];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int c = warp; c < K; c += nw) tab_build_warp(tabs[c], d_rs ? d_rs[c] : rs.v[c], lane);
+    if (threadIdx.x < KH + KL) r[threadIdx.x] = d_rs ? d_rs[threadIdx.x] : rs.v[threadIdx.x];
+    __syncthreads();
+    // evaluate_lagrange_basis (src/utils.rs:4-27) of each half: entry j has
+    // r where j's bit is set and 1 + r where not, the half's first challenge
+    // on j's top bit
+    for (int t = warp; t < NL + NH; t += nw) {
+        const bool lo = t < NL;
+        const int j = lo ? t : t - NL, nb = lo ? KL : KH, off = lo ? KH : 0;
+        uint32_t e = 1;
+        for (int b = 0; b < nb; ++b) e = gf_mul(e, ((j >> (nb - 1 - b)) & 1) ? r[off + b] : 1u ^ r[off + b]);
+        tab_build_warp(tabs[t], e, lane);
+    }
     __syncthreads();
     const uint8_t *t8 = reinterpret_cast<const uint8_t *>(&tabs[0][0]);
-    constexpr int NJ = 1 << K, RUN = NJ < 8 ? NJ : 8;
-    const uint64_t groups = M / V;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t *src = in + g * V;
-        VecV<V> st[K + 1];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t acc = 0;
 #pragma unroll
-        for (int j0 = 0; j0 < NJ; j0 += RUN) {
-            VecV<V> leaf[RUN];
+        for (int jh = 0; jh < NH; ++jh) {
+            uint32_t v[NL];
 #pragma unroll
-            for (int u = 0; u < RUN; ++u) leaf[u] = load_v<V>(src + (uint64_t)(j0 + u) * M);
+            for (int jl = 0; jl < NL; ++jl) v[jl] = __ldg(in + (uint64_t)(jh * NL + jl) * M + i);
+            uint32_t part = 0;
 #pragma unroll
-            for (int u = 0; u < RUN; ++u) {
-                const int j = j0 + u;
-                VecV<V> cur = leaf[u];
-                int c = 0;
-#pragma unroll
-                for (; c < K && ((j >> c) & 1); ++c) {
-                    // level c pairs j's bit c: left = st[c], right = cur,
-                    // challenge rs[K-1-c] (table K-1-c)
-#pragma unroll
-                    for (int v = 0; v < V; ++v)
-                        cur.x[v] = st[c].x[v] ^ tab_mul_sa(t8, 512u * (K - 1 - c), 0, st[c].x[v] ^ cur.x[v]);
-                }
-                st[c] = cur;
-            }
+            for (int jl = 0; jl < NL; ++jl) part ^= tab_mul_sa(t8, 512u * jl, 0, v[jl]);
+            acc ^= KH ? tab_mul_sa(t8, 512u * (NL + jh), 0, part) : part;
         }
-        if constexpr (V == 4) {
-            *reinterpret_cast<uint4 *>(out + g * 4) = make_uint4(st[K].x[0], st[K].x[1], st[K].x[2], st[K].x[3]);
-        } else {
-#pragma unroll
-            for (int v = 0; v < V; ++v) out[g * V + v] = st[K].x[v];
-        }
+        out[i] = acc;
     }
 }
 
@@ -957,14 +958,14 @@ cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log
     if (!d_rs)
         for (uint32_t j = 0; j < k; ++j) c.v[j] = rs[j];
     const uint64_t M = 1ull << (log_len - k);
-    const bool vec4 = M % 4 == 0 && ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
-    const uint64_t groups = vec4 ? M / 4 : M;
-    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * 8));
-    L.note(4.0 * (M << k) + 4.0 * M, (double)M * ((1u << k) - 1));
-    switch (k * 2 + (vec4 ? 1 : 0)) {
-#define LGK_CASE(kk)                                                                                              \
-    case 2 * kk: LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_tree<kk, 1>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); break; \
-    case 2 * kk + 1: LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_tree<kk, 4>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); break;
+    const uint32_t kh = k / 2;
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((M + 255) / 256, 148ull * 6));
+    L.note(4.0 * (M << k) + 4.0 * M, (double)M * ((1u << k) + (kh ? (1u << kh) : 0)));
+    switch (k) {
+#define LGK_CASE(kk)                                                                                         \
+    case kk:                                                                                                 \
+        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); \
+        break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
     }
@@ -1158,27 +1159,38 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
 // is entry u - 2^h times S_k[h] (Lo; Hi from apow_k and S_k[b + h]), one
 // product per entry and a block barrier per bit.  Block 0 also XORs the
 // queries' contributions into the enforced sum.
+// The doubling runs in shared memory when Lo and Hi fit (in_smem), one
+// barrier per level, and the finished vectors are written out coalesced;
+// larger ones double in place in global memory.
 __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__restrict__ apow, uint32_t n,
                               uint32_t b, uint32_t nq, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi,
-                              uint32_t *sum_out) {
+                              uint32_t *sum_out, int in_smem) {
     pdl_begin();
-    const uint32_t k = blockIdx.x;
+    extern __shared__ uint32_t sbuf[];  // Lo then Hi, when in_smem
+    __shared__ uint32_t Ss[32];          // the query's subspace values, read once
+    const uint32_t k = blockIdx.x, nlo = 1u << b, nhi = 1u << (n - b);
     const uint32_t *Sk = S + (uint64_t)k * n;
-    uint32_t *lk = lo + ((uint64_t)k << b), *hk = hi + ((uint64_t)k << (n - b));
+    uint32_t *glk = lo + ((uint64_t)k << b), *ghk = hi + ((uint64_t)k << (n - b));
+    uint32_t *lk = in_smem ? sbuf : glk, *hk = in_smem ? sbuf + nlo : ghk;
+    if (threadIdx.x < n && threadIdx.x < 32) Ss[threadIdx.x] = Sk[threadIdx.x];
     if (threadIdx.x == 0) {
         lk[0] = 1;
         hk[0] = apow[k];
     }
     __syncthreads();
     for (uint32_t h = 0; h < b; ++h) {
-        const uint32_t s = Sk[h];
+        const uint32_t s = Ss[h];
         for (uint32_t u = threadIdx.x; u < (1u << h); u += blockDim.x) lk[(1u << h) + u] = gf_mul(lk[u], s);
         __syncthreads();
     }
     for (uint32_t h = 0; h < n - b; ++h) {
-        const uint32_t s = Sk[b + h];
+        const uint32_t s = Ss[b + h];
         for (uint32_t c = threadIdx.x; c < (1u << h); c += blockDim.x) hk[(1u << h) + c] = gf_mul(hk[c], s);
         __syncthreads();
+    }
+    if (in_smem) {
+        for (uint32_t u = threadIdx.x; u < nlo; u += blockDim.x) glk[u] = lk[u];
+        for (uint32_t c = threadIdx.x; c < nhi; c += blockDim.x) ghk[c] = hk[c];
     }
     if (k == 0 && threadIdx.x < 32) {
         uint32_t x = 0;
@@ -1248,8 +1260,10 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
                          uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum) {
     const double vec = (double)nq * ((1ull << p.b) + (1ull << (n - p.b)));  // Lo and Hi words
     L.note(4.0 * vec, vec);
-    LGK_LAUNCH(L, "induce_prep",
-               launch_k(k_induce_prep, nq, 256, 0, L.stream, d_S, d_apow, n, p.b, nq, d_lo, d_hi, d_sum));
+    const size_t words = (1ull << p.b) + (1ull << (n - p.b));
+    const int in_smem = words <= 12288;  // 48 KB: no opt-in needed
+    LGK_LAUNCH(L, "induce_prep", launch_k(k_induce_prep, nq, 256, in_smem ? 4 * words : 0, L.stream, d_S, d_apow, n,
+                                          p.b, nq, d_lo, d_hi, d_sum, in_smem));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dim3 grid(1u << (n - p.b), p.qsplit);
