@@ -286,8 +286,7 @@ struct Witness {  // RecursiveLigeroWitness, src/data_structures.rs:32-40
 // quarters reads them from there, instead of spreading four copies through
 // HBM; codes short enough for a single FFT pass spread them.
 void rs_encode(lg_ctx *c, const Code &code, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *E,
-               uint64_t col_stride, uint32_t *scaled, lgk::FftPasses passes = lgk::FFT_ALL,
-               const lgk::TailHash *hash = nullptr) {
+               uint64_t col_stride, uint32_t *scaled, lgk::FftPasses passes = lgk::FFT_ALL) {
     const uint64_t m = 1ull << log_m;
     if (log_m > 6) {
         CK(c, lgk::rs_scale(c->L, d_poly, code.pis, scaled, log_m, n));
@@ -295,34 +294,23 @@ void rs_encode(lg_ctx *c, const Code &code, const uint32_t *d_poly, uint32_t log
         src.p = scaled;
         src.col_stride = m;
         src.q_stride = 0;
-        CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, col_stride, 4, m, 4, false, passes, &src, hash));
+        CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, col_stride, 4, m, 4, false, passes, &src));
     } else {
         CK(c, lgk::rs_scale_spread(c->L, d_poly, code.pis, E, log_m, n));
-        CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, col_stride, 4, m, 4, false, passes, nullptr, hash));
+        CK(c, lgk::fft_vectors(c->L, E, code.tw, log_m, n, col_stride, 4, m, 4, false, passes));
     }
 }
 
-// ligero_commit (src/ligero.rs:70-95) into caller buffers.  When every
-// column fits one tile of the last FFT pass, that pass also hashes the
-// leaves and the 6 layers above them (each 64-row tile is a subtree), and
-// only the tree's top remains.
+// ligero_commit (src/ligero.rs:70-95) into caller buffers
 void commit_into(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n, uint32_t *E, uint32_t *tree) {
     const Code code = get_code(c, log_m);
     const uint64_t m = 1ull << log_m, rows = 4 * m;
-    const bool fused = lgk::tail_hash_fusable(log_m, n) && (uintptr_t)E % 16 == 0 && (uintptr_t)tree % 16 == 0;
-    lgk::TailHash th;
-    th.tree = tree;
-    th.leaves = rows;
     {
         DBuf scaled(c, log_m > 6 ? 4ull * n * m : 0);
-        rs_encode(c, code, d_poly, log_m, n, E, rows, scaled.u32(), lgk::FFT_ALL, fused ? &th : nullptr);
+        rs_encode(c, code, d_poly, log_m, n, E, rows, scaled.u32());
     }
-    if (fused) {
-        CK(c, lgk::merkle_upper_from(c->L, tree, rows, 6));
-    } else {
-        CK(c, lgk::leaf_hashes(c->L, E, rows, n, tree));
-        CK(c, lgk::merkle_upper(c->L, tree, rows));
-    }
+    CK(c, lgk::leaf_hashes(c->L, E, rows, n, tree));
+    CK(c, lgk::merkle_upper(c->L, tree, rows));
 }
 
 Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {

@@ -73,33 +73,6 @@ bool pdl_enabled() {
 
 static inline unsigned ilog2u(uint64_t x) { unsigned r = 0; while (x > 1) { x >>= 1; ++r; } return r; }
 
-// Node = blake3(left || right): one 64-byte block, CHUNK_START|CHUNK_END|ROOT
-// (src/merkle_tree.rs:42-51).
-__device__ __forceinline__ void hash_node(const uint32_t *l, const uint32_t *r, uint32_t *o, uint32_t one) {
-    uint32_t m[16];
-#pragma unroll
-    for (int w = 0; w < 8; ++w) { m[w] = l[w]; m[8 + w] = r[w]; }
-    uint32_t cv[8];
-    b3_iv(cv);
-    b3_compress(cv, m, 64, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT, one);
-#pragma unroll
-    for (int w = 0; w < 8; ++w) o[w] = cv[w];
-}
-
-__device__ __forceinline__ void load_node(const uint32_t *p, uint32_t (&h)[8]) {
-    const uint4 x = reinterpret_cast<const uint4 *>(p)[0], y = reinterpret_cast<const uint4 *>(p)[1];
-    h[0] = x.x; h[1] = x.y; h[2] = x.z; h[3] = x.w; h[4] = y.x; h[5] = y.y; h[6] = y.z; h[7] = y.w;
-}
-__device__ __forceinline__ void store_node(uint32_t *p, const uint32_t (&h)[8]) {
-    reinterpret_cast<uint4 *>(p)[0] = make_uint4(h[0], h[1], h[2], h[3]);
-    reinterpret_cast<uint4 *>(p)[1] = make_uint4(h[4], h[5], h[6], h[7]);
-}
-__device__ __forceinline__ void hash_pair(const uint32_t (&l)[8], const uint32_t (&r)[8], uint32_t (&o)[8],
-                                          uint32_t one) {
-    hash_node(l, r, o, one);
-}
-
-
 // ====================================================== RS scale + spread
 __global__ void k_rs_scale_spread(const uint32_t *__restrict__ poly, const uint32_t *__restrict__ pis,
                                   uint32_t *__restrict__ E, uint32_t log_m, uint64_t total) {
@@ -228,9 +201,6 @@ struct PassArgs {
     uint64_t units;            // strided passes: (group, chunk) work units
     const uint32_t *src;       // strided passes: input, when not data (FftSrc)
     uint64_t src_col_stride, src_q_stride;
-    uint32_t *tree;            // last pass: Merkle tree to start (TailHash), or null
-    uint64_t leaves;
-    uint32_t one;              // 1 (a runtime operand for BLAKE3's additions)
 };
 
 // The 2^K - 1 node tables of one (q, P), in 512-byte slots at the start of
@@ -410,15 +380,7 @@ __global__ void __launch_bounds__(256, K <= 4 ? 4 : (K == 5 ? 4 : 2)) k_fft_pass
 // run over vectors, so a warp shares every table it reads; the block has
 // as many threads as a phase has pencils (up to 256), so a tile of few
 // vectors still keeps every thread busy.
-//
-// HASH (forward, K = 6, all of a row's columns in the tile): the tile then
-// holds 64 whole rows of the encoded matrix, i.e. 64 consecutive leaves
-// (src/ligero.rs:53-68), so the block also hashes them (BLAKE3 over each
-// row's words, src/merkle_tree.rs:4-20) and climbs their 6-layer subtree
-// (src/merkle_tree.rs:38-57), writing every node: the leaf pass over the
-// matrix and the tree's wide layers need no launch or HBM read of their
-// own.  Two warps hash while the others store the tile.
-template <int K, bool INV, bool HASH>
+template <int K, bool INV>
 __global__ void __launch_bounds__(256, 4) k_fft_tail(PassArgs a) {
     pdl_begin();
     constexpr int KA = K / 2, KB = K - KA, RB = 1 << KB, R = 1 << K, STRIDE = R + 1, CPC = R / 4;
@@ -480,64 +442,11 @@ __global__ void __launch_bounds__(256, 4) k_fft_tail(PassArgs a) {
     }
     __syncthreads();
 
-    uint32_t first = 0, step = blockDim.x;  // threads that store the tile
-    if constexpr (HASH) {
-        static_assert(K == 6, "a tile is a 64-leaf subtree");
-        constexpr uint32_t NH = 64;  // hashing threads: one per row, then per node
-        // node buffers in the table area, which the stages no longer need
-        uint32_t *ha = reinterpret_cast<uint32_t *>(smraw), *hb = ha + 8 * NH;
-        const uint64_t leaf0 = (uint64_t)q * a.q_stride + ((uint64_t)P << K);
-        if (threadIdx.x < NH) {
-            const uint32_t t = threadIdx.x, nb = (nvec + 15) / 16;
-            uint32_t cv[8];
-            b3_iv(cv);
-            for (uint32_t b = 0; b < nb; ++b) {
-                uint32_t m[16];
-#pragma unroll
-                for (int w = 0; w < 16; ++w) {
-                    const uint32_t j = b * 16 + w;
-                    m[w] = j < nvec ? tile[j * STRIDE + t] : 0u;
-                }
-                const bool last = b + 1 == nb;
-                const uint32_t blen = last ? 4 * nvec - 64 * (nb - 1) : 64;
-                const uint32_t flags = (b == 0 ? B3_CHUNK_START : 0u) | (last ? (B3_CHUNK_END | B3_ROOT) : 0u);
-                b3_compress(cv, m, blen, flags, a.one);
-            }
-            store_node(a.tree + 8 * (leaf0 + t), cv);
-#pragma unroll
-            for (int w = 0; w < 8; ++w) ha[8 * t + w] = cv[w];
-            // the subtree's layers, one named barrier (the hashing warps
-            // only) per layer
-            uint64_t off = 0, width = a.leaves;
-            uint32_t *src = ha, *dst = hb;
-            for (uint32_t lvl = 1; lvl <= K; ++lvl) {
-                asm volatile("bar.sync 1, 64;" ::: "memory");
-                off += width;
-                width >>= 1;
-                const uint32_t cnt = NH >> lvl;
-                if (t < cnt) {
-                    uint32_t l[8], r[8], h[8];
-#pragma unroll
-                    for (int w = 0; w < 8; ++w) { l[w] = src[16 * t + w]; r[w] = src[16 * t + 8 + w]; }
-                    hash_pair(l, r, h, a.one);
-                    store_node(a.tree + 8 * (off + (leaf0 >> lvl) + t), h);
-#pragma unroll
-                    for (int w = 0; w < 8; ++w) dst[8 * t + w] = h[w];
-                }
-                uint32_t *tp = src;
-                src = dst;
-                dst = tp;
-            }
-        }
-        if (blockDim.x > NH) first = NH, step = blockDim.x - NH;
-        else __syncthreads();
+    for (uint32_t c = threadIdx.x; c < nvec * CPC; c += blockDim.x) {
+        const uint32_t j = c / CPC, piece = c % CPC;
+        const uint32_t *d = tile + j * STRIDE + 4 * piece;
+        *reinterpret_cast<uint4 *>(gbase + j * a.col_stride + 4 * piece) = make_uint4(d[0], d[1], d[2], d[3]);
     }
-    if (threadIdx.x >= first)
-        for (uint32_t c = threadIdx.x - first; c < nvec * CPC; c += step) {
-            const uint32_t j = c / CPC, piece = c % CPC;
-            const uint32_t *d = tile + j * STRIDE + 4 * piece;
-            *reinterpret_cast<uint4 *>(gbase + j * a.col_stride + 4 * piece) = make_uint4(d[0], d[1], d[2], d[3]);
-        }
 }
 
 static size_t pass_smem(int K) { return (size_t)((1 << K) - 1) * 512; }
@@ -588,8 +497,7 @@ static cudaError_t launch_pass(Launcher &L, int K, PassArgs a, unsigned threads)
 template <bool INV>
 static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) {
     char nmbuf[48];
-    std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_tail" : (a.tree ? "fft_tail_hash" : "fft_tail"),
-                  a.L, K, a.nvec);
+    std::snprintf(nmbuf, sizeof nmbuf, "%s_L%u_K%d_n%u", INV ? "ifft_tail" : "fft_tail", a.L, K, a.nvec);
     const size_t smem = tail_smem(K, a.vchunk);
     // the kernel's limit is always set to its largest tile: contexts on other
     // threads launch the same kernel with other tile sizes, and a smaller
@@ -599,17 +507,11 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
     while (vp2 < a.vchunk) vp2 <<= 1;
     // pencils per phase: vectors x 2^(K - K/2) (the larger phase)
     const unsigned threads = std::max<unsigned>(32, std::min<unsigned>(256, vp2 << (K - K / 2)));
-    if (a.tree) {
-        if (INV || K != 6 || a.nchunks != 1 || threads < 64) return cudaErrorInvalidValue;
-        cudaFuncSetAttribute(k_fft_tail<6, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
-        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_tail<6, false, true>, blocks, threads, smem, L.stream, a));
-        return cudaGetLastError();
-    }
     switch (K) {
 #define LGK_CASE(k)                                                                                 \
     case k:                                                                                         \
-        cudaFuncSetAttribute(k_fft_tail<k, INV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max); \
-        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_tail<k, INV, false>, blocks, threads, smem, L.stream, a));         \
+        cudaFuncSetAttribute(k_fft_tail<k, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);   \
+        LGK_LAUNCH(L, nmbuf, launch_k(k_fft_tail<k, INV>, blocks, threads, smem, L.stream, a));           \
         break;
         LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
@@ -618,20 +520,11 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
     return cudaGetLastError();
 }
 
-bool tail_hash_fusable(uint32_t log_len, uint32_t nvec) {
-    // the last pass takes 6 stages in 64-row tiles holding every column, and
-    // has at least two warps (vectors x 8 pencils per phase)
-    return log_len >= 6 && nvec >= 8 && nvec <= 64;
-}
-
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
-                        uint32_t root_base, bool inverse, FftPasses passes, const FftSrc *src,
-                        const TailHash *hash) {
+                        uint32_t root_base, bool inverse, FftPasses passes, const FftSrc *src) {
     if (log_len == 0 || nvec == 0) return cudaSuccess;
     if (inverse && passes != FFT_ALL) return cudaErrorInvalidValue;
-    if (hash && (inverse || passes == FFT_HEAD || !tail_hash_fusable(log_len, nvec) || !hash->tree))
-        return cudaErrorInvalidValue;
     if (src && (inverse || log_len <= 6 || passes == FFT_LAST)) return cudaErrorInvalidValue;
     // the roots root_base + q (q < Q) must share one heap layer
     const uint32_t lr = 31 - __builtin_clz(root_base);
@@ -681,13 +574,9 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
         a.src = (src && p == 0) ? src->p : nullptr;
         a.src_col_stride = src ? src->col_stride : 0;
         a.src_q_stride = src ? src->q_stride : 0;
-        a.tree = (hash && p == np - 1) ? hash->tree : nullptr;
-        a.leaves = hash ? hash->leaves : 0;
-        a.one = 1;
         a.L = log_len; a.d0 = d0; a.log_S = log_len - d0 - K;
         a.log_nvec_p2 = ilog2u(nvec_p2); a.nvec = nvec; a.root_base = root_base;
         const bool tail = a.log_S == 0 && K >= 4 && aligned;
-        if (a.tree && !tail) return cudaErrorInvalidValue;
         {
             // every vector read (the source once when all Q subtrees share
             // it) and written once; one product per butterfly and stage
@@ -793,11 +682,38 @@ cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t 
     return cudaGetLastError();
 }
 
+// Node = blake3(left || right): one 64-byte block, CHUNK_START|CHUNK_END|ROOT
+// (src/merkle_tree.rs:42-51).  A block reduces 2^c consecutive nodes of one
+// layer through c layers in shared memory and writes every layer it makes.
+__device__ __forceinline__ void hash_node(const uint32_t *l, const uint32_t *r, uint32_t *o, uint32_t one) {
+    uint32_t m[16];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) { m[w] = l[w]; m[8 + w] = r[w]; }
+    uint32_t cv[8];
+    b3_iv(cv);
+    b3_compress(cv, m, 64, B3_CHUNK_START | B3_CHUNK_END | B3_ROOT, one);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) o[w] = cv[w];
+}
+
 // The tree is stored leaves first, layer after layer, 8 words per node.
 // Wide layers: a thread takes 8 consecutive nodes (256 contiguous bytes)
 // and hashes the 7 nodes of the three layers above them, keeping at most
 // three pending hashes; every lane does full work, so these launches run
 // at hashing throughput.
+__device__ __forceinline__ void load_node(const uint32_t *p, uint32_t (&h)[8]) {
+    const uint4 x = reinterpret_cast<const uint4 *>(p)[0], y = reinterpret_cast<const uint4 *>(p)[1];
+    h[0] = x.x; h[1] = x.y; h[2] = x.z; h[3] = x.w; h[4] = y.x; h[5] = y.y; h[6] = y.z; h[7] = y.w;
+}
+__device__ __forceinline__ void store_node(uint32_t *p, const uint32_t (&h)[8]) {
+    reinterpret_cast<uint4 *>(p)[0] = make_uint4(h[0], h[1], h[2], h[3]);
+    reinterpret_cast<uint4 *>(p)[1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+__device__ __forceinline__ void hash_pair(const uint32_t (&l)[8], const uint32_t (&r)[8], uint32_t (&o)[8],
+                                          uint32_t one) {
+    hash_node(l, r, o, one);
+}
+
 __global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
                                                         uint32_t one) {
     pdl_begin();
@@ -916,14 +832,8 @@ __global__ void __launch_bounds__(256) k_merkle_narrow(uint32_t *__restrict__ tr
 }
 
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
-    return merkle_upper_from(L, tree, num_leaves, 0);
-}
-
-cudaError_t merkle_upper_from(Launcher &L, uint32_t *tree, uint64_t num_leaves, uint32_t level) {
-    if (num_leaves == 0 || (num_leaves & (num_leaves - 1)) || !L.tickets || (num_leaves >> level) == 0)
-        return cudaErrorInvalidValue;
+    if (num_leaves == 0 || (num_leaves & (num_leaves - 1)) || !L.tickets) return cudaErrorInvalidValue;
     uint64_t off = 0, n = num_leaves;
-    for (uint32_t l = 0; l < level; ++l) { off += n; n >>= 1; }
     // Three layers per launch with a thread per 8 nodes while a layer has
     // more than 2^18 nodes (every lane does full work); from a layer of
     // 2^18 or fewer, one launch climbs to the root.

@@ -118,22 +118,10 @@ struct FftSrc {
     const uint32_t *p = nullptr;
     uint64_t col_stride = 0, q_stride = 0;
 };
-// hash: the forward transform's last pass also starts the Merkle tree of
-// the matrix the vectors form (vector j = column j, rows along the
-// vectors: row index = q * q_stride + position, q_stride in rows): every
-// leaf (BLAKE3 of a row's nvec words) and the 6 layers above the leaves,
-// into tree (all layers, leaves first, 8 words per node, `leaves` rows);
-// merkle_upper_from(.., 6) finishes it.  Needs tail_hash_fusable and every
-// column of the matrix in one call.
-struct TailHash {
-    uint32_t *tree = nullptr;
-    uint64_t leaves = 0;
-};
-bool tail_hash_fusable(uint32_t log_len, uint32_t nvec);
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
                         uint32_t root_base, bool inverse, FftPasses passes = FFT_ALL,
-                        const FftSrc *src = nullptr, const TailHash *hash = nullptr);
+                        const FftSrc *src = nullptr);
 
 // --- Merkle (src/merkle_tree.rs:4-60, leaves src/ligero.rs:53-68) --------
 // Leaf hash of every row of a column-major matrix (rows x ncols u32).
@@ -147,8 +135,6 @@ cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint3
 // All upper layers from the leaf layer at tree[0]; tree as 8-word nodes.
 // Needs the Launcher's tickets.
 cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves);
-// The same from the layer `level` up (the layers below already written).
-cudaError_t merkle_upper_from(Launcher &L, uint32_t *tree, uint64_t num_leaves, uint32_t level);
 
 // --- gathers for openings (src/ligero.rs:40-51, src/merkle_tree.rs:98) ---
 // out = the nq opened rows (nq x ncols words), then count Merkle nodes (8
