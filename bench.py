@@ -330,7 +330,8 @@ def run_ours(args):
             # proofs batched vs looped, and a served Poisson stream vs a FIFO
             # loop at matched p99 (10,000 requests per offered rate)
             line["batch64"] = batch64(lg, 3, 1)
-            line["serve"] = serve_sweep(lg, 10000, [1000, 2000, 4000, 8000], 8)
+            line["serve"] = serve_sweep(lg, 10000, [1000, 2000, 3000, 4000, 5000, 6000, 8000], 8,
+                                        fifo_rates=[1000, 2000, 3000, 4000])
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -557,7 +558,7 @@ def run_batch64(args):
     print(json.dumps(batch64(g.load_package(), args.steps, args.warmup)), flush=True)
 
 
-def serve_sweep(lg, n_req: int, rates, workers: int, log=None) -> dict:
+def serve_sweep(lg, n_req: int, rates, workers: int, log=None, fifo_rates=None) -> dict:
     """Poisson arrivals of proof requests, log sizes in {16..24} with
     P(s) ~ 2^(-(s-16)/2), coefficients SplitMix64 seed 4+i generated on the
     device as each request arrives, 160 GB admission budget.  The FIFO loop
@@ -581,7 +582,7 @@ def serve_sweep(lg, n_req: int, rates, workers: int, log=None) -> dict:
     for nw in (1, workers):
         srv = lg.Server(0, workers=nw, hbm_budget_bytes=budget)
         srv.warm([cfg_by[int(L)] for L in svals])
-        for rate in rates:
+        for rate in (fifo_rates or rates) if nw == 1 else rates:
             gaps = np.random.default_rng(int(rate)).exponential(1.0 / rate, size=n_req)
             lat, keep, tickets = [], {}, []
             lock = threading.Lock()

@@ -116,15 +116,34 @@ __device__ __forceinline__ void tab_build_warp(uint32_t *T, uint32_t c, int lane
 // constant after unrolling.  Byte j of a (b) holds 4 * nibble 2j (2j+1) of
 // w, the byte offset of that window's entry; one byte-permute splices it
 // under `base`, and off + the window's 64-byte slot fold into the load's
-// immediate.  Per product: 4 ops to spread the nibbles, 8 permutes, 8
-// loads, 4 XORs.
+// immediate.  Per product: 2 multiplies and 2 ANDs to spread the nibbles, 8
+// permutes, 8 loads, 4 XORs.
+// p + t * stride_bytes as one wide multiply-add on the multiply-add pipe
+// (the strided FFT passes address 2^K pencil values this way, keeping the
+// integer-logic pipe for the field products)
+template <class T>
+__device__ __forceinline__ T *strided(T *p, uint32_t t, uint32_t stride_bytes) {
+    T *r;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(t), "r"(stride_bytes), "l"(p));
+    return r;
+}
+
 __device__ __forceinline__ uint32_t shared_addr(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
+// The two nibble spreads' shifts run as multiplies on the multiply-add pipe
+// (w * 4, and the high word of w * 2^30 = w >> 2): a table product is
+// otherwise all integer-logic work (the byte permutes and XORs), and that
+// pipe is what bounds the table kernels.  The multipliers come from
+// constant memory so the compiler keeps them multiplies.
+static __constant__ uint32_t kSpreadMul[2] = {4u, 1u << 30};
 __device__ __forceinline__ uint32_t tab_mul_sa(const uint8_t *__restrict__ sm, uint32_t base, uint32_t off,
                                                uint32_t w) {
-    const uint32_t a = (w << 2) & 0x3C3C3C3Cu;
-    const uint32_t b = (w >> 2) & 0x3C3C3C3Cu;
+    uint32_t a, b;
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(a) : "r"(w), "r"(kSpreadMul[0]));
+    asm("mul.hi.u32 %0, %1, %2;" : "=r"(b) : "r"(w), "r"(kSpreadMul[1]));
+    a &= 0x3C3C3C3Cu;
+    b &= 0x3C3C3C3Cu;
 #define LGD_LD(x, sel, o) (*reinterpret_cast<const uint32_t *>(sm + __byte_perm((x), base, (sel)) + off + (o)))
     const uint32_t r0 = LGD_LD(a, 0x7650, 0), r1 = LGD_LD(b, 0x7650, 64);
     const uint32_t r2 = LGD_LD(a, 0x7651, 128), r3 = LGD_LD(b, 0x7651, 192);

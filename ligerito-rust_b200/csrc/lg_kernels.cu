@@ -109,6 +109,7 @@ __global__ void k_rs_scale(const uint32_t *__restrict__ poly, const uint32_t *__
 // the current one, so its HBM latency hides behind the table builds and
 // lookups.
 constexpr uint32_t kScaleRows = 32, kScaleCols = 64, kScaleThreads = 256;
+static_assert(kScaleCols == 64 && kScaleRows % (kScaleThreads / 32) == 0, "two column halves per lane");
 constexpr uint32_t kScalePer = kScaleRows * kScaleCols / kScaleThreads;  // words per thread
 __global__ void __launch_bounds__(kScaleThreads) k_rs_scale_tab(const uint32_t *__restrict__ poly,
                                                                 const uint32_t *__restrict__ pis,
@@ -130,23 +131,52 @@ __global__ void __launch_bounds__(kScaleThreads) k_rs_scale_tab(const uint32_t *
             pre[i] = j < ncol ? __ldg(poly + (uint64_t)(j0 + j) * m + i0 + r) : 0u;
         }
     };
+    // each warp builds the tables of rows warp + 8 rr (rr < 4); their pis
+    // words are loaded a tile ahead with the data
+    constexpr uint32_t kRowsPerWarp = kScaleRows / (kScaleThreads / 32);
+    uint32_t pc[kRowsPerWarp], pn[kRowsPerWarp];
+    auto load_pis = [&](uint32_t t, uint32_t (&dst)[kRowsPerWarp]) {
+#pragma unroll
+        for (uint32_t rr = 0; rr < kRowsPerWarp; ++rr)
+            dst[rr] = __ldg(pis + (uint64_t)t * kScaleRows + warp + (kScaleThreads / 32) * rr);
+    };
     uint32_t t = blockIdx.x;
-    if (t < ntiles) load(t);
+    if (t < ntiles) {
+        load(t);
+        load_pis(t, pc);
+    }
     for (; t < ntiles; t += gridDim.x) {
         const uint64_t i0 = (uint64_t)t * kScaleRows;
-        for (uint32_t r = warp; r < kScaleRows; r += kScaleThreads / 32)
-            tab_build_warp(tabs[r], __ldg(pis + i0 + r), lane);
+#pragma unroll
+        for (uint32_t rr = 0; rr < kRowsPerWarp; ++rr)
+            tab_build_warp(tabs[warp + (kScaleThreads / 32) * rr], pc[rr], lane);
 #pragma unroll
         for (uint32_t i = 0; i < kScalePer; ++i) {
             const uint32_t c = threadIdx.x + kScaleThreads * i;
             tile[(c / kScaleRows) * (kScaleRows + 1) + c % kScaleRows] = pre[i];
         }
         __syncthreads();
-        if (t + gridDim.x < ntiles) load(t + gridDim.x);  // in flight during the lookups
-        for (uint32_t r = warp; r < kScaleRows; r += kScaleThreads / 32)
-            for (uint32_t j = lane; j < ncol; j += 32) {
-                uint32_t *x = tile + j * (kScaleRows + 1) + r;
-                *x = tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * r, 0, *x);
+        if (t + gridDim.x < ntiles) {  // in flight during the lookups
+            load(t + gridDim.x);
+            load_pis(t + gridDim.x, pn);
+        }
+        // 8 independent products per lane: rows warp + 8 rr, columns lane + 32 jj
+        uint32_t x[kRowsPerWarp][2];
+#pragma unroll
+        for (uint32_t rr = 0; rr < kRowsPerWarp; ++rr)
+#pragma unroll
+            for (uint32_t jj = 0; jj < 2; ++jj) {
+                const uint32_t j = lane + 32 * jj, r = warp + (kScaleThreads / 32) * rr;
+                x[rr][jj] = j < ncol ? tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * r, 0,
+                                                  tile[j * (kScaleRows + 1) + r])
+                                     : 0u;
+            }
+#pragma unroll
+        for (uint32_t rr = 0; rr < kRowsPerWarp; ++rr)
+#pragma unroll
+            for (uint32_t jj = 0; jj < 2; ++jj) {
+                const uint32_t j = lane + 32 * jj, r = warp + (kScaleThreads / 32) * rr;
+                if (j < ncol) tile[j * (kScaleRows + 1) + r] = x[rr][jj];
             }
         __syncthreads();
 #pragma unroll
@@ -154,6 +184,8 @@ __global__ void __launch_bounds__(kScaleThreads) k_rs_scale_tab(const uint32_t *
             const uint32_t c = threadIdx.x + kScaleThreads * i, j = c / kScaleRows, r = c % kScaleRows;
             if (j < ncol) out[(uint64_t)(j0 + j) * m + i0 + r] = tile[j * (kScaleRows + 1) + r];
         }
+#pragma unroll
+        for (uint32_t rr = 0; rr < kRowsPerWarp; ++rr) pc[rr] = pn[rr];
         __syncthreads();  // the tile and tables are rewritten next
     }
 }
@@ -302,6 +334,7 @@ __global__ void __launch_bounds__(256, K <= 4 ? 4 : (K == 5 ? 4 : 2)) k_fft_pass
     const uint32_t U = (uint32_t)a.units, nb = gridDim.x;
     const uint32_t u0 = (uint32_t)((uint64_t)blockIdx.x * U / nb), u1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * U / nb);
     const uint64_t S = 1ull << a.log_S;
+    const uint32_t S4 = 4u << a.log_S;  // bytes between pencil values (a vector is < 4 GiB)
     uint32_t cur = 0xFFFFFFFFu;
     const bool own_src = a.src != nullptr;
     const uint64_t scs = own_src ? a.src_col_stride : a.col_stride;
@@ -325,7 +358,7 @@ __global__ void __launch_bounds__(256, K <= 4 ? 4 : (K == 5 ? 4 : 2)) k_fft_pass
     bool have = PF && u0 < u1 && locate(u0, lb, sb);
     if (PF && have) {
 #pragma unroll
-        for (int t = 0; t < NP; ++t) nv[t] = lb[t * S];
+        for (int t = 0; t < NP; ++t) nv[t] = *strided(lb, (uint32_t)t, S4);
     }
     for (uint32_t u = u0; u < u1; ++u) {
         const uint32_t grp = u >> a.log_bpg;
@@ -345,14 +378,14 @@ __global__ void __launch_bounds__(256, K <= 4 ? 4 : (K == 5 ? 4 : 2)) k_fft_pass
             have = u + 1 < u1 && locate(u + 1, lb, sb);
             if (have) {
 #pragma unroll
-                for (int t = 0; t < NP; ++t) nv[t] = lb[t * S];
+                for (int t = 0; t < NP; ++t) nv[t] = *strided(lb, (uint32_t)t, S4);
             }
         } else {
             mine = locate(u, lb, sb);
             base = sb;
             if (mine) {
 #pragma unroll
-                for (int t = 0; t < (1 << K); ++t) v[t] = lb[t * S];
+                for (int t = 0; t < (1 << K); ++t) v[t] = *strided(lb, (uint32_t)t, S4);
             }
         }
         if (!mine) continue;
@@ -366,7 +399,7 @@ __global__ void __launch_bounds__(256, K <= 4 ? 4 : (K == 5 ? 4 : 2)) k_fft_pass
             for (int t = 0; t < (1 << K); ++t) base[t * S2] = v[t];
         } else {
 #pragma unroll
-            for (int t = 0; t < (1 << K); ++t) base[t * S] = v[t];
+            for (int t = 0; t < (1 << K); ++t) *strided(base, (uint32_t)t, S4) = v[t];
         }
     }
 }
@@ -909,11 +942,12 @@ __device__ __forceinline__ uint32_t lagrange_at(const uint32_t *rs, uint32_t k, 
 // out[i] = sum_jh EH[jh] * (sum_jl EL[jl] * in[(jh 2^kl + jl) M + i]): the
 // inner sums take 2^k products over 2^kl tables shared by every lane, the
 // outer 2^kh more over 2^kh tables.  A block builds its 2^kl + 2^kh tables
-// once and then loops over outputs; every product in an inner sum is
-// independent of the others, so loads and lookups overlap.
+// once and then loops over outputs, four consecutive ones per thread (one
+// 16-byte load per term); every product in an inner sum is independent of
+// the others, so loads and lookups overlap.
 struct Rs6 { uint32_t v[6]; };
 
-template <int KH, int KL>
+template <int KH, int KL, int V>
 __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
                                                  uint64_t M, Rs6 rs, const uint32_t *d_rs) {
     pdl_begin();
@@ -935,19 +969,42 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
     }
     __syncthreads();
     const uint8_t *t8 = reinterpret_cast<const uint8_t *>(&tabs[0][0]);
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t acc = 0;
+    // V consecutive outputs per thread (16-byte loads for V = 4)
+    const uint64_t groups = M / V;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t *src = in + g * V;
+        uint32_t acc[V];
+#pragma unroll
+        for (int x = 0; x < V; ++x) acc[x] = 0;
 #pragma unroll
         for (int jh = 0; jh < NH; ++jh) {
-            uint32_t v[NL];
+            uint32_t v[NL][V];
 #pragma unroll
-            for (int jl = 0; jl < NL; ++jl) v[jl] = __ldg(in + (uint64_t)(jh * NL + jl) * M + i);
-            uint32_t part = 0;
+            for (int jl = 0; jl < NL; ++jl) {
+                const uint32_t *p = src + (uint64_t)(jh * NL + jl) * M;
+                if constexpr (V == 4) {
+                    const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+                    v[jl][0] = t.x; v[jl][1] = t.y; v[jl][2] = t.z; v[jl][3] = t.w;
+                } else {
 #pragma unroll
-            for (int jl = 0; jl < NL; ++jl) part ^= tab_mul_sa(t8, 512u * jl, 0, v[jl]);
-            acc ^= KH ? tab_mul_sa(t8, 512u * (NL + jh), 0, part) : part;
+                    for (int x = 0; x < V; ++x) v[jl][x] = __ldg(p + x);
+                }
+            }
+#pragma unroll
+            for (int x = 0; x < V; ++x) {
+                uint32_t part = 0;
+#pragma unroll
+                for (int jl = 0; jl < NL; ++jl) part ^= tab_mul_sa(t8, 512u * jl, 0, v[jl][x]);
+                acc[x] ^= KH ? tab_mul_sa(t8, 512u * (NL + jh), 0, part) : part;
+            }
         }
-        out[i] = acc;
+        if constexpr (V == 4) {
+            *reinterpret_cast<uint4 *>(out + g * 4) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+        } else {
+#pragma unroll
+            for (int x = 0; x < V; ++x) out[g * V + x] = acc[x];
+        }
     }
 }
 
@@ -959,12 +1016,17 @@ cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log
         for (uint32_t j = 0; j < k; ++j) c.v[j] = rs[j];
     const uint64_t M = 1ull << (log_len - k);
     const uint32_t kh = k / 2;
-    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((M + 255) / 256, 148ull * 6));
+    const bool vec4 = M % 4 == 0 && (uintptr_t)in % 16 == 0 && (uintptr_t)out % 16 == 0;
+    const uint64_t groups = vec4 ? M / 4 : M;
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * 4));
     L.note(4.0 * (M << k) + 4.0 * M, (double)M * ((1u << k) + (kh ? (1u << kh) : 0)));
-    switch (k) {
-#define LGK_CASE(kk)                                                                                         \
-    case kk:                                                                                                 \
-        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); \
+    switch (2 * k + (vec4 ? 1 : 0)) {
+#define LGK_CASE(kk)                                                                                          \
+    case 2 * kk:                                                                                              \
+        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2, 1>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); \
+        break;                                                                                                \
+    case 2 * kk + 1:                                                                                          \
+        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2, 4>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); \
         break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
