@@ -92,6 +92,15 @@ const char *lg_ctx_last_error(const lg_ctx *ctx);
 void *lg_ctx_stream(lg_ctx *ctx);        /* the cudaStream_t every call is issued on */
 lg_status lg_ctx_synchronize(lg_ctx *ctx);
 uint64_t lg_ctx_launch_count(const lg_ctx *ctx); /* kernels this context launched */
+/* Autotuning (off by default; LG_AUTOTUNE=1 in the environment turns it on
+ * for new contexts): with it on, the first whole FFT of a shape (length,
+ * vectors, subtrees) and the first fold of a shape time their candidate
+ * stage splits / grids on scratch buffers and keep the fastest for the
+ * process, every context of the device.  Every choice gives the same
+ * results.  lg_tuned_choices lists the choices made, one per line (buf
+ * NULL: *len = the size with its NUL).  No reference counterpart. */
+lg_status lg_ctx_set_autotune(lg_ctx *ctx, int enabled);
+lg_status lg_tuned_choices(char *buf, uint64_t *len);
 /* Per-kernel CUDA-event timing (off by default); stats accumulate until reset. */
 lg_status lg_ctx_set_kernel_timing(lg_ctx *ctx, int enabled);
 lg_status lg_ctx_kernel_stats(lg_ctx *ctx, uint32_t index, char *name, size_t name_cap,

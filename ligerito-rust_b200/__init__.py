@@ -100,6 +100,8 @@ def _load() -> ctypes.CDLL:
         "lg_ctx_kernel_stats": (i32, [P, u32, ctypes.c_char_p, ctypes.c_size_t, P, P]),
         "lg_ctx_reset_kernel_stats": (i32, [P]),
         "lg_ctx_kernel_work": (i32, [P, u32, P, P, P]),
+        "lg_ctx_set_autotune": (i32, [P, i32]),
+        "lg_tuned_choices": (i32, [P, P]),
         "lg_measure_pipe_peaks": (i32, [i32, P, u32]),
         "lg_ctx_device_bytes_in_use": (u64, [P]),
         "lg_ctx_device_bytes_cached": (u64, [P]),
@@ -402,12 +404,24 @@ class Context:
             i += 1
         return out
 
+    def set_autotune(self, enabled: bool) -> None:
+        _check(lib.lg_ctx_set_autotune(self.handle, 1 if enabled else 0), self)
+
     def reset_kernel_stats(self) -> None:
         _check(lib.lg_ctx_reset_kernel_stats(self.handle), self)
 
     @property
     def device_bytes_in_use(self) -> int:
         return int(lib.lg_ctx_device_bytes_in_use(self.handle))
+
+
+def tuned_choices() -> list:
+    """The autotuner's choices so far (lg_tuned_choices), one string each."""
+    n = ctypes.c_uint64()
+    _check(lib.lg_tuned_choices(None, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value)
+    _check(lib.lg_tuned_choices(buf, ctypes.byref(n)))
+    return [x for x in buf.value.decode().splitlines() if x]
 
 
 PIPES = ("lop3", "iadd", "prmt", "shf", "imad", "imad_hi", "lop3_imad", "lds")

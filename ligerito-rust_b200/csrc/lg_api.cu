@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -1232,6 +1233,11 @@ lg_status lg_ctx_create(int device, uint64_t budget, lg_ctx **out) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     c->L.stream = c->stream;
+    c->L.device = device;
+    {
+        const char *e = std::getenv("LG_AUTOTUNE");
+        c->L.autotune = e && e[0] == '1';
+    }
     {
         std::lock_guard<std::mutex> lk(g_tables_mu);
         ++g_tables[device].contexts;
@@ -1272,6 +1278,20 @@ lg_status lg_ctx_synchronize(lg_ctx *c) {
     return guarded(c, [&] { sync(c); });
 }
 uint64_t lg_ctx_launch_count(const lg_ctx *c) { return c ? c->L.launches : 0; }
+lg_status lg_ctx_set_autotune(lg_ctx *c, int on) {
+    if (!c) return LG_ERR_INVALID_ARGUMENT;
+    c->L.autotune = on != 0;
+    return LG_OK;
+}
+lg_status lg_tuned_choices(char *buf, uint64_t *len) {
+    if (!len) return LG_ERR_INVALID_ARGUMENT;
+    const std::string s = lgk::tuned_choices();
+    if (!buf) { *len = s.size() + 1; return LG_OK; }
+    if (*len < s.size() + 1) { *len = s.size() + 1; return LG_ERR_INVALID_ARGUMENT; }
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    *len = s.size() + 1;
+    return LG_OK;
+}
 lg_status lg_ctx_set_kernel_timing(lg_ctx *c, int on) {
     if (!c) return LG_ERR_INVALID_ARGUMENT;
     c->L.timing = on != 0;

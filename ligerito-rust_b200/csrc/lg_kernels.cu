@@ -8,6 +8,9 @@
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
 
 using namespace lgd;
 
@@ -553,6 +556,33 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
     return cudaGetLastError();
 }
 
+// Stage split: the last pass (register phases over shared-memory tiles,
+// many warps per SM) takes up to 6 stages; the strided passes before it
+// hold a 2^K-value pencil per thread, and K = 4-5 keeps twice the warps per
+// SM of K = 6 (measured faster per stage) while still doing several stages
+// per trip through HBM.  The autotuner may replace it per shape.
+FftPlan default_fft_plan(uint32_t log_len) {
+    FftPlan pl;
+    const uint32_t kt = std::min<uint32_t>(6, log_len), rem = log_len - kt;
+    const uint32_t nps = rem == 0 ? 0 : (rem <= 6 ? 1 : (rem + 4) / 5);
+    pl.np = nps + 1;
+    for (uint32_t i = 0; i < nps && i < kMaxFftPasses; ++i) pl.ks[i] = rem / nps + (i < rem % nps ? 1 : 0);
+    if (nps < kMaxFftPasses) pl.ks[nps] = kt;
+    return pl;
+}
+
+static bool plan_valid(const FftPlan &pl, uint32_t log_len) {
+    if (pl.np == 0 || pl.np > kMaxFftPasses) return false;
+    uint32_t sum = 0;
+    for (uint32_t i = 0; i < pl.np; ++i) {
+        if (pl.ks[i] < 1 || pl.ks[i] > 6) return false;
+        sum += pl.ks[i];
+    }
+    // the last pass runs in tiles when it has 4..6 stages; strided passes
+    // before it need at least one level below them
+    return sum == log_len;
+}
+
 cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_t log_len,
                         uint32_t nvec, uint64_t col_stride, uint32_t Q, uint64_t q_stride,
                         uint32_t root_base, bool inverse, FftPasses passes, const FftSrc *src) {
@@ -562,22 +592,26 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
     // the roots root_base + q (q < Q) must share one heap layer
     const uint32_t lr = 31 - __builtin_clz(root_base);
     if (!L.dtab || root_base == 0 || ((root_base + Q - 1) >> lr) != 1) return cudaErrorInvalidValue;
-    // Stage split: the last pass (register phases over shared-memory
-    // tiles, 32 registers, many warps per SM) takes up to 6 stages; the
-    // strided passes before it hold a 2^K-value pencil per thread, and
-    // K = 4-5 keeps twice the warps per SM of K = 6 (measured faster per
-    // stage) while still doing several stages per trip through HBM.
-    const uint32_t kt = std::min<uint32_t>(6, log_len), rem = log_len - kt;
-    const uint32_t nps = rem == 0 ? 0 : (rem <= 6 ? 1 : (rem + 4) / 5);
-    const uint32_t np = nps + 1;
-    if (np > kMaxFftPasses) return cudaErrorInvalidValue;
-    std::vector<uint32_t> ks(np, kt);
-    for (uint32_t i = 0; i < nps; ++i) ks[i] = rem / nps + (i < rem % nps ? 1 : 0);
+    // head / last calls on column groups must agree on the split, so only
+    // whole transforms take tuned plans
+    FftPlan plan = default_fft_plan(log_len);
+    if (passes == FFT_ALL && !L.forced_plan) {
+        const TuneKey tk{L.device, log_len, nvec, Q, src != nullptr, inverse, 0};
+        if (!tuned_fft_plan(tk, &plan) && L.autotune) {
+            cudaError_t e = tune_fft(L, tk, data, tw, col_stride, q_stride, root_base, src, &plan);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    if (L.forced_plan) plan = *L.forced_plan;
+    if (!plan_valid(plan, log_len)) return cudaErrorInvalidValue;
+    const uint32_t np = plan.np;
+    std::vector<uint32_t> ks(plan.ks, plan.ks + np);
     std::vector<uint32_t> d0s(np);
     for (uint32_t i = 0, d = 0; i < np; ++i) { d0s[i] = d; d += ks[i]; }
     // D tables of every pass; kept while the same twiddle subtree is asked
-    // for again (the twiddle arrays live, unchanged, as long as the context)
-    const Launcher::DtabKey key{tw, log_len, root_base};
+    // for again with the same split (the twiddle arrays live, unchanged, as
+    // long as the context)
+    const Launcher::DtabKey key{tw, log_len, root_base, plan_code(plan)};
     uint32_t slot = 0;
     while (slot < kDtabSlots && !(L.dtab_key[slot] == key)) ++slot;
     if (slot == kDtabSlots) {
@@ -1008,6 +1042,9 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
     }
 }
 
+static bool tuned_fold(const TuneKey &k, int *bps);
+static void tune_fold(Launcher &L, const TuneKey &k, const uint32_t *rs, const uint32_t *d_rs);
+
 cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
                     const uint32_t *rs, const uint32_t *d_rs) {
     if (k < 1 || k > 6 || k > log_len || (!rs && !d_rs)) return cudaErrorInvalidValue;
@@ -1018,7 +1055,19 @@ cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log
     const uint32_t kh = k / 2;
     const bool vec4 = M % 4 == 0 && (uintptr_t)in % 16 == 0 && (uintptr_t)out % 16 == 0;
     const uint64_t groups = vec4 ? M / 4 : M;
-    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * 4));
+    // blocks per SM: tuned per shape (4 by default)
+    int bps = 4;
+    if (L.forced_fold_bps) {
+        bps = L.forced_fold_bps;
+    } else {
+        const TuneKey tk{L.device, log_len, k, 1, false, false, 1};
+        if (!tuned_fold(tk, &bps)) {
+            if (L.autotune) tune_fold(L, tk, rs, d_rs);
+            if (!tuned_fold(tk, &bps)) bps = 4;
+        }
+    }
+    const unsigned blocks =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * (uint64_t)bps));
     L.note(4.0 * (M << k) + 4.0 * M, (double)M * ((1u << k) + (kh ? (1u << kh) : 0)));
     switch (2 * k + (vec4 ? 1 : 0)) {
 #define LGK_CASE(kk)                                                                                          \
@@ -1532,6 +1581,194 @@ cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n) {
     L.note(4.0 * n, 0);
     LGK_LAUNCH(L, "splitmix", launch_k(k_splitmix, blocks, 256, 0, L.stream, seed, out, n));
     return cudaGetLastError();
+}
+
+// ============================================================= autotuner
+bool TuneKey::operator<(const TuneKey &o) const {
+    auto t = [](const TuneKey &k) { return std::make_tuple(k.device, k.kind, k.log_len, k.nvec, k.Q, k.src, k.inverse); };
+    return t(*this) < t(o);
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::map<TuneKey, FftPlan> g_fft_plans;
+std::map<TuneKey, int> g_fold_bps;
+
+// Candidate splits: the last pass 4-6 stages, the strided passes before it
+// 3-6 each (at most kMaxFftPasses passes), the default first.
+std::vector<FftPlan> fft_candidates(uint32_t log_len) {
+    std::vector<FftPlan> out{default_fft_plan(log_len)};
+    if (log_len <= 6) return out;
+    auto add = [&](const FftPlan &p) {
+        for (auto &q : out)
+            if (plan_code(q) == plan_code(p)) return;
+        out.push_back(p);
+    };
+    for (uint32_t kt = 6; kt >= 4; --kt) {
+        const uint32_t rem = log_len - kt;
+        for (uint32_t nps = 1; nps < kMaxFftPasses && nps <= rem; ++nps) {
+            if (rem > 6 * nps || rem < 3 * nps) continue;
+            // even split (larger first) and with the larger passes last
+            FftPlan a, b;
+            a.np = b.np = nps + 1;
+            for (uint32_t i = 0; i < nps; ++i) {
+                a.ks[i] = rem / nps + (i < rem % nps ? 1 : 0);
+                b.ks[nps - 1 - i] = a.ks[i];
+            }
+            a.ks[nps] = b.ks[nps] = kt;
+            add(a);
+            add(b);
+        }
+    }
+    if (out.size() > 10) out.resize(10);
+    return out;
+}
+}  // namespace
+
+bool tuned_fft_plan(const TuneKey &k, FftPlan *out) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_fft_plans.find(k);
+    if (it == g_fft_plans.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+// Times every candidate split of this transform shape on scratch buffers
+// of the same extent (the values do not change the work), keeps the
+// fastest for the process and returns it.  Buffers that cannot be
+// allocated leave the default split, untuned.
+cudaError_t tune_fft(Launcher &L, const TuneKey &k, uint32_t *data, const uint32_t *tw, uint64_t col_stride,
+                     uint64_t q_stride, uint32_t root_base, const FftSrc *src, FftPlan *out) {
+    (void)data;
+    const uint64_t n = 1ull << k.log_len;
+    const uint64_t extent = (uint64_t)(k.nvec - 1) * col_stride + (uint64_t)(k.Q - 1) * q_stride + n;
+    const uint64_t src_extent = src ? (uint64_t)(k.nvec - 1) * src->col_stride + (uint64_t)(k.Q - 1) * src->q_stride + n : 0;
+    uint32_t *sd = nullptr, *ss = nullptr;
+    if (cudaMallocAsync(&sd, 4 * extent, L.stream) != cudaSuccess ||
+        (src && cudaMallocAsync(&ss, 4 * src_extent, L.stream) != cudaSuccess)) {
+        cudaGetLastError();
+        if (sd) cudaFreeAsync(sd, L.stream);
+        *out = default_fft_plan(k.log_len);
+        return cudaSuccess;
+    }
+    FftSrc s2;
+    if (src) { s2 = *src; s2.p = ss; }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const bool timing = L.timing;
+    L.timing = false;
+    FftPlan best = default_fft_plan(k.log_len);
+    float best_ms = 1e30f;
+    cudaError_t err = cudaSuccess;
+    for (const FftPlan &c : fft_candidates(k.log_len)) {
+        L.forced_plan = &c;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3 && err == cudaSuccess; ++rep) {
+            cudaEventRecord(a, L.stream);
+            err = fft_vectors(L, sd, tw, k.log_len, k.nvec, col_stride, k.Q, q_stride, root_base, k.inverse, FFT_ALL,
+                              src ? &s2 : nullptr);
+            cudaEventRecord(b, L.stream);
+            cudaEventSynchronize(b);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, a, b);
+            if (rep > 0) ms = std::min(ms, t);  // the first run builds the split's tables
+        }
+        L.forced_plan = nullptr;
+        if (err != cudaSuccess) break;
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    L.forced_plan = nullptr;
+    L.timing = timing;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFreeAsync(sd, L.stream);
+    if (ss) cudaFreeAsync(ss, L.stream);
+    if (err != cudaSuccess) return err;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_fft_plans[k] = best;
+    }
+    *out = best;
+    return cudaSuccess;
+}
+
+static bool tuned_fold(const TuneKey &k, int *bps) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_fold_bps.find(k);
+    if (it == g_fold_bps.end()) return false;
+    *bps = it->second;
+    return true;
+}
+
+// Times the fold grid at 1, 2, 3 and 4 blocks per SM on scratch buffers
+// and keeps the fastest (nothing is recorded if they cannot be allocated).
+static void tune_fold(Launcher &L, const TuneKey &k, const uint32_t *rs, const uint32_t *d_rs) {
+    const uint64_t n = 1ull << k.log_len;
+    uint32_t *in = nullptr, *out = nullptr, *drs = nullptr;
+    if (cudaMallocAsync(&in, 4 * n, L.stream) != cudaSuccess ||
+        cudaMallocAsync(&out, 4 * (n >> k.nvec) + 16, L.stream) != cudaSuccess ||
+        cudaMallocAsync(&drs, 64, L.stream) != cudaSuccess) {
+        cudaGetLastError();
+        if (in) cudaFreeAsync(in, L.stream);
+        if (out) cudaFreeAsync(out, L.stream);
+        return;
+    }
+    // the challenges' values do not change the work
+    cudaMemsetAsync(drs, 0x5A, 64, L.stream);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const bool timing = L.timing;
+    L.timing = false;
+    int best = 4;
+    float best_ms = 1e30f;
+    for (int bps = 1; bps <= 4; ++bps) {
+        L.forced_fold_bps = bps;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(a, L.stream);
+            fold_eq(L, in, out, k.log_len, k.nvec, nullptr, drs);
+            cudaEventRecord(b, L.stream);
+            cudaEventSynchronize(b);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, a, b);
+            if (rep > 0) ms = std::min(ms, t);
+        }
+        if (ms < best_ms) { best_ms = ms; best = bps; }
+    }
+    L.forced_fold_bps = 0;
+    L.timing = timing;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFreeAsync(in, L.stream);
+    cudaFreeAsync(out, L.stream);
+    cudaFreeAsync(drs, L.stream);
+    (void)rs;
+    (void)d_rs;
+    if (cudaGetLastError() != cudaSuccess) return;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_fold_bps[k] = best;
+}
+
+std::string tuned_choices() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::string s;
+    char buf[160];
+    for (auto &kv : g_fft_plans) {
+        std::snprintf(buf, sizeof buf, "fft device %d log_len %u vectors %u subtrees %u src %d inverse %d : passes",
+                      kv.first.device, kv.first.log_len, kv.first.nvec, kv.first.Q, (int)kv.first.src,
+                      (int)kv.first.inverse);
+        s += buf;
+        for (uint32_t i = 0; i < kv.second.np; ++i) s += " " + std::to_string(kv.second.ks[i]);
+        s += "\n";
+    }
+    for (auto &kv : g_fold_bps) {
+        std::snprintf(buf, sizeof buf, "fold device %d log_len %u k %u : blocks/SM %d\n", kv.first.device,
+                      kv.first.log_len, kv.first.nvec, kv.second);
+        s += buf;
+    }
+    return s;
 }
 
 }  // namespace lgk

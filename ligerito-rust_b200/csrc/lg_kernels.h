@@ -20,8 +20,26 @@ constexpr size_t kDtabWords = kMaxFftPasses * 63 * 128;
 // commitments), so a steady run of proofs builds none
 constexpr uint32_t kDtabSlots = 4;
 
+// A stage split of an FFT: np passes of ks[i] stages, the last one in tiles.
+struct FftPlan {
+    uint32_t np = 0;
+    uint32_t ks[kMaxFftPasses] = {};
+};
+inline uint32_t plan_code(const FftPlan &p) {  // a compact key (3 bits a pass)
+    uint32_t c = p.np;
+    for (uint32_t i = 0; i < p.np && i < kMaxFftPasses; ++i) c = c * 8 + p.ks[i];
+    return c;
+}
+
 struct Launcher {
     cudaStream_t stream = nullptr;
+    int device = 0;
+    // Autotuning (see tune_fft / tuned_fold_blocks): when set, the first call
+    // of a shape times the candidates on scratch buffers and keeps the
+    // fastest for the process; forced_plan overrides the split (tuning runs).
+    bool autotune = false;
+    const FftPlan *forced_plan = nullptr;
+    int forced_fold_bps = 0;
     // device scratch of kDtabSlots x kDtabWords, owned by the context: sets
     // of the FFT passes' shared twiddle tables (fft_vectors), rebuilt in
     // stream order, each with the twiddle subtree it was built for and its
@@ -32,8 +50,10 @@ struct Launcher {
     uint32_t *tickets = nullptr;
     struct DtabKey {
         const uint32_t *tw = nullptr;
-        uint32_t log_len = 0, root_base = 0;
-        bool operator==(const DtabKey &o) const { return tw == o.tw && log_len == o.log_len && root_base == o.root_base; }
+        uint32_t log_len = 0, root_base = 0, plan = 0;
+        bool operator==(const DtabKey &o) const {
+            return tw == o.tw && log_len == o.log_len && root_base == o.root_base && plan == o.plan;
+        }
     } dtab_key[kDtabSlots];
     uint64_t dtab_used[kDtabSlots] = {}, dtab_clock = 0;
     uint64_t launches = 0;
@@ -87,6 +107,25 @@ cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t sme
         __VA_ARGS__;               \
         (L).end(name, _ev);        \
     } while (0)
+
+// --- autotuner -------------------------------------------------------------
+// Choices measured on this device and kept for the process (all contexts):
+// the FFT stage split per transform shape, and the fold grid.  Every choice
+// computes the same values (the split only regroups the same butterflies),
+// so tuning changes speed only.
+struct TuneKey {
+    int device;
+    uint32_t log_len, nvec, Q;
+    bool src, inverse;
+    uint32_t kind;  // 0 FFT, 1 fold
+    bool operator<(const TuneKey &o) const;
+};
+FftPlan default_fft_plan(uint32_t log_len);
+bool tuned_fft_plan(const TuneKey &k, FftPlan *out);
+cudaError_t tune_fft(Launcher &L, const TuneKey &k, uint32_t *data, const uint32_t *tw, uint64_t col_stride,
+                     uint64_t q_stride, uint32_t root_base, const struct FftSrc *src, FftPlan *out);
+// "log_len nvec Q src inv : k0 k1 ..." lines, and "fold log_len k : blocks/SM"
+std::string tuned_choices();
 
 // --- Reed-Solomon column encoding (src/reed_solomon.rs:104-113) ----------
 // E (column-major, n columns of 4m): every quarter of column j receives
