@@ -221,6 +221,8 @@ def run_ours(args):
     dev = local
     torch.cuda.set_device(dev)
     ctx = lg.Context(dev)
+    # the first warm-up proof tunes the FFT splits and the fold grid
+    ctx.set_autotune(not args.no_autotune)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=f"cuda:{dev}")
     pipes = lg.measure_pipe_peaks(dev)
     cfg = lg.hardcoded_config_24()
@@ -324,6 +326,7 @@ def run_ours(args):
             "clocks": clocks,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "autotune": lg.tuned_choices(),
         }
         if world == 1 and not args.no_mixed:
             # the mixed-size forms against the plain GPU prover: 64 uneven
@@ -657,6 +660,7 @@ def main():
     ap.add_argument("--requests", type=int, default=10000, help="serve: number of requests per rate")
     ap.add_argument("--rates", default="1000,2000,3000,4000,6000,8000", help="serve: offered rates (requests/s)")
     ap.add_argument("--no-mixed", action="store_true", help="prove24: skip the batch64 / serve objects")
+    ap.add_argument("--no-autotune", action="store_true", help="prove24: default FFT splits and fold grid")
     ap.add_argument("--workers", type=int, default=8, help="serve: concurrent workers")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -407,86 +407,112 @@ __global__ void __launch_bounds__(256, K <= 4 ? 4 : (K == 5 ? 4 : 2)) k_fft_pass
     }
 }
 
-// Last pass (contiguous blocks of 2^K rows): one block per (q, P) tile of
-// 2^K rows x nvec vectors.  The tile is loaded with coalesced 16-byte reads
-// into shared memory with an odd column stride (2^K + 1 words), so both a
-// lane-per-vector walk down a column and a lane-per-row walk across the
-// columns are bank-conflict free.  All warps build the 2^K - 1 tables, then
-// the stages run in two register phases of about K/2 stages each.  Lanes
-// run over vectors, so a warp shares every table it reads; the block has
-// as many threads as a phase has pencils (up to 256), so a tile of few
-// vectors still keeps every thread busy.
+// Last pass (contiguous blocks of 2^K rows): one block per (q, P), which
+// builds that group's 2^K - 1 node tables once and then walks the vectors
+// in chunks of vchunk (<= 32), double-buffered: the next chunk is copied
+// into shared memory asynchronously (cp.async) while the current one runs
+// its stages, so the tile loads' HBM latency hides behind the lookups (the
+// first chunk's behind the table builds).  A chunk's tile has an odd column
+// stride (2^K + 1 words), so both a lane-per-vector walk down a column and
+// a lane-per-row walk across the columns are bank-conflict free.  The
+// stages run in two register phases of about K/2 stages each; lanes run
+// over vectors, so a warp shares every table it reads.
+__device__ __forceinline__ void cp_async4(uint32_t *dst, const uint32_t *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(shared_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 template <int K, bool INV>
 __global__ void __launch_bounds__(256, 4) k_fft_tail(PassArgs a) {
     pdl_begin();
-    constexpr int KA = K / 2, KB = K - KA, RB = 1 << KB, R = 1 << K, STRIDE = R + 1, CPC = R / 4;
+    constexpr int KA = K / 2, KB = K - KA, RB = 1 << KB, R = 1 << K, STRIDE = R + 1;
     extern __shared__ __align__(16) uint8_t smraw[];
-    const unsigned chunk = blockIdx.x % a.nchunks, rest = blockIdx.x / a.nchunks;
-    const unsigned P = rest & ((1u << a.d0) - 1);
-    const unsigned q = rest >> a.d0;
-    const uint32_t nvec = min(a.vchunk, a.nvec - chunk * a.vchunk);
-    build_pass_tables<K>(smraw, a, q, P);
-    const uint32_t tb = 0;
-    uint32_t *tile = reinterpret_cast<uint32_t *>(smraw + tb + ((1 << K) - 1) * 512);
-    uint32_t *gbase = a.data + (uint64_t)chunk * a.vchunk * a.col_stride + q * a.q_stride + ((uint64_t)P << K);
-
-    for (uint32_t c = threadIdx.x; c < nvec * CPC; c += blockDim.x) {
-        const uint32_t j = c / CPC, piece = c % CPC;
-        const uint4 x = *reinterpret_cast<const uint4 *>(gbase + j * a.col_stride + 4 * piece);
-        uint32_t *d = tile + j * STRIDE + 4 * piece;
-        d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w;
-    }
-    __syncthreads();
-
-    // Two register phases: KA stages on pencils of 2^KA values at stride
-    // 2^KB, then KB stages on contiguous pencils of 2^KB values.  Work items
-    // run over (vector, pencil) with the vector index in the low bits (a
-    // power-of-two span, so the split is a mask and a shift).
-    const uint32_t lnv = 32 - __clz(nvec - 1), vmask = (1u << lnv) - 1;
-    auto phase_a = [&]() {
-        for (uint32_t item = threadIdx.x; item < ((uint32_t)RB << lnv); item += blockDim.x) {
-            const uint32_t j = item & vmask, u = item >> lnv;
-            if (j >= nvec) continue;
-            uint32_t v[1 << KA];
-#pragma unroll
-            for (int i = 0; i < (1 << KA); ++i) v[i] = tile[j * STRIDE + u + RB * i];
-            pencil_stages<KA, 0, INV>(v, smraw, tb, 0);
-#pragma unroll
-            for (int i = 0; i < (1 << KA); ++i) tile[j * STRIDE + u + RB * i] = v[i];
+    const unsigned P = blockIdx.x & ((1u << a.d0) - 1);
+    const unsigned q = blockIdx.x >> a.d0;
+    uint32_t *const tile0 = reinterpret_cast<uint32_t *>(smraw + ((1 << K) - 1) * 512);
+    const uint32_t tile_words = a.vchunk * STRIDE;  // buffer b at tile0 + b * tile_words
+    const uint32_t *gsrc = a.data + q * a.q_stride + ((uint64_t)P << K);
+    uint32_t *gdst = a.data + q * a.q_stride + ((uint64_t)P << K);
+    // chunk c's vectors [c vchunk, c vchunk + nv)
+    auto chunk_len = [&](uint32_t c) { return min(a.vchunk, a.nvec - c * a.vchunk); };
+    auto load_chunk = [&](uint32_t c, uint32_t *tile) {
+        const uint32_t nv = chunk_len(c);
+        const uint32_t *g = gsrc + (uint64_t)c * a.vchunk * a.col_stride;
+        for (uint32_t e = threadIdx.x; e < nv * R; e += blockDim.x) {
+            const uint32_t j = e / R, r = e % R;
+            cp_async4(tile + j * STRIDE + r, g + j * a.col_stride + r);
         }
+        cp_async_commit();
     };
-    auto phase_b = [&]() {
-        for (uint32_t item = threadIdx.x; item < ((1u << KA) << lnv); item += blockDim.x) {
-            const uint32_t j = item & vmask, gq = item >> lnv;
-            if (j >= nvec) continue;
-            uint32_t v[RB];
-#pragma unroll
-            for (int i = 0; i < RB; ++i) v[i] = tile[j * STRIDE + RB * gq + i];
-            pencil_stages<KB, KA, INV>(v, smraw, tb, gq);
-#pragma unroll
-            for (int i = 0; i < RB; ++i) tile[j * STRIDE + RB * gq + i] = v[i];
+    load_chunk(0, tile0);
+    build_pass_tables<K>(smraw, a, q, P);  // ends with the block synchronised
+    const uint32_t nchunks = a.nchunks;
+    for (uint32_t c = 0; c < nchunks; ++c) {
+        uint32_t *tile = tile0 + (c & 1) * tile_words;
+        const uint32_t nvec = chunk_len(c);
+        if (c + 1 < nchunks) {
+            load_chunk(c + 1, tile0 + ((c + 1) & 1) * tile_words);
+            cp_async_wait<1>();  // chunk c has landed (the one after may be in flight)
+        } else {
+            cp_async_wait<0>();
         }
-    };
-    if (!INV) {
-        phase_a();
         __syncthreads();
-        phase_b();
-    } else {
-        phase_b();
-        __syncthreads();
-        phase_a();
-    }
-    __syncthreads();
 
-    for (uint32_t c = threadIdx.x; c < nvec * CPC; c += blockDim.x) {
-        const uint32_t j = c / CPC, piece = c % CPC;
-        const uint32_t *d = tile + j * STRIDE + 4 * piece;
-        *reinterpret_cast<uint4 *>(gbase + j * a.col_stride + 4 * piece) = make_uint4(d[0], d[1], d[2], d[3]);
+        // Two register phases: KA stages on pencils of 2^KA values at stride
+        // 2^KB, then KB stages on contiguous pencils of 2^KB values.  Work
+        // items run over (vector, pencil) with the vector index in the low
+        // bits (a power-of-two span, so the split is a mask and a shift).
+        const uint32_t lnv = 32 - __clz(nvec - 1), vmask = (1u << lnv) - 1;
+        auto phase_a = [&]() {
+            for (uint32_t item = threadIdx.x; item < ((uint32_t)RB << lnv); item += blockDim.x) {
+                const uint32_t j = item & vmask, u = item >> lnv;
+                if (j >= nvec) continue;
+                uint32_t v[1 << KA];
+#pragma unroll
+                for (int i = 0; i < (1 << KA); ++i) v[i] = tile[j * STRIDE + u + RB * i];
+                pencil_stages<KA, 0, INV>(v, smraw, 0, 0);
+#pragma unroll
+                for (int i = 0; i < (1 << KA); ++i) tile[j * STRIDE + u + RB * i] = v[i];
+            }
+        };
+        auto phase_b = [&]() {
+            for (uint32_t item = threadIdx.x; item < ((1u << KA) << lnv); item += blockDim.x) {
+                const uint32_t j = item & vmask, gq = item >> lnv;
+                if (j >= nvec) continue;
+                uint32_t v[RB];
+#pragma unroll
+                for (int i = 0; i < RB; ++i) v[i] = tile[j * STRIDE + RB * gq + i];
+                pencil_stages<KB, KA, INV>(v, smraw, 0, gq);
+#pragma unroll
+                for (int i = 0; i < RB; ++i) tile[j * STRIDE + RB * gq + i] = v[i];
+            }
+        };
+        if (!INV) {
+            phase_a();
+            __syncthreads();
+            phase_b();
+        } else {
+            phase_b();
+            __syncthreads();
+            phase_a();
+        }
+        __syncthreads();
+        uint32_t *g = gdst + (uint64_t)c * a.vchunk * a.col_stride;
+        constexpr int CPC = R / 4;  // 16-byte pieces per column
+        for (uint32_t e = threadIdx.x; e < nvec * CPC; e += blockDim.x) {
+            const uint32_t j = e / CPC, piece = e % CPC;
+            const uint32_t *d = tile + j * STRIDE + 4 * piece;
+            *reinterpret_cast<uint4 *>(g + j * a.col_stride + 4 * piece) = make_uint4(d[0], d[1], d[2], d[3]);
+        }
+        __syncthreads();  // this buffer takes chunk c + 2 next
     }
 }
 
+constexpr uint32_t kTailChunk = 32;  // vectors per tile of the last pass
 static size_t pass_smem(int K) { return (size_t)((1 << K) - 1) * 512; }
-static size_t tail_smem(int K, uint32_t nvec) { return pass_smem(K) + (size_t)nvec * ((1u << K) + 1) * 4; }
+static size_t tail_smem(int K, uint32_t vchunk) { return pass_smem(K) + 2 * (size_t)vchunk * ((1u << K) + 1) * 4; }
 
 // One wave of strided-pass blocks: as many as fit on the device at once
 // (occupancy of this instantiation, cached), at most one per unit.
@@ -538,7 +564,7 @@ static cudaError_t launch_tail(Launcher &L, int K, PassArgs a, unsigned blocks) 
     // the kernel's limit is always set to its largest tile: contexts on other
     // threads launch the same kernel with other tile sizes, and a smaller
     // limit set between another thread's set and launch would fail it
-    const int smem_max = (int)tail_smem(K, 64);
+    const int smem_max = (int)tail_smem(K, kTailChunk);
     uint32_t vp2 = 1;
     while (vp2 < a.vchunk) vp2 <<= 1;
     // pencils per phase: vectors x 2^(K - K/2) (the larger phase)
@@ -652,9 +678,9 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
             L.note(4.0 * (rd + words), words / 2 * K);
         }
         if (tail) {
-            a.vchunk = std::min<uint32_t>(nvec, 64);
+            a.vchunk = std::min<uint32_t>(nvec, kTailChunk);
             a.nchunks = (nvec + a.vchunk - 1) / a.vchunk;
-            const uint64_t blocks = ((uint64_t)Q << d0) * a.nchunks;
+            const uint64_t blocks = (uint64_t)Q << d0;  // one per group; chunks run inside it
             if (blocks > 0x7FFFFFFFull) return cudaErrorInvalidValue;
             cudaError_t e = inverse ? launch_tail<true>(L, (int)K, a, (unsigned)blocks)
                                     : launch_tail<false>(L, (int)K, a, (unsigned)blocks);
@@ -1053,19 +1079,22 @@ cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log
         for (uint32_t j = 0; j < k; ++j) c.v[j] = rs[j];
     const uint64_t M = 1ull << (log_len - k);
     const uint32_t kh = k / 2;
-    const bool vec4 = M % 4 == 0 && (uintptr_t)in % 16 == 0 && (uintptr_t)out % 16 == 0;
-    const uint64_t groups = vec4 ? M / 4 : M;
-    // blocks per SM: tuned per shape (4 by default)
-    int bps = 4;
+    // grid choice: blocks per SM in the low byte, bit 8 for four outputs
+    // per thread; tuned per shape (one output per thread, 4 blocks per SM
+    // by default)
+    int choice = 4;
     if (L.forced_fold_bps) {
-        bps = L.forced_fold_bps;
+        choice = L.forced_fold_bps;
     } else {
         const TuneKey tk{L.device, log_len, k, 1, false, false, 1};
-        if (!tuned_fold(tk, &bps)) {
+        if (!tuned_fold(tk, &choice)) {
             if (L.autotune) tune_fold(L, tk, rs, d_rs);
-            if (!tuned_fold(tk, &bps)) bps = 4;
+            if (!tuned_fold(tk, &choice)) choice = 4;
         }
     }
+    const int bps = choice & 0xFF;
+    const bool vec4 = (choice & 0x100) && M % 4 == 0 && (uintptr_t)in % 16 == 0 && (uintptr_t)out % 16 == 0;
+    const uint64_t groups = vec4 ? M / 4 : M;
     const unsigned blocks =
         (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * (uint64_t)bps));
     L.note(4.0 * (M << k) + 4.0 * M, (double)M * ((1u << k) + (kh ? (1u << kh) : 0)));
@@ -1701,8 +1730,9 @@ static bool tuned_fold(const TuneKey &k, int *bps) {
     return true;
 }
 
-// Times the fold grid at 1, 2, 3 and 4 blocks per SM on scratch buffers
-// and keeps the fastest (nothing is recorded if they cannot be allocated).
+// Times the fold grid at 1, 2, 3 and 4 blocks per SM, one or four outputs
+// per thread, on scratch buffers and keeps the fastest (nothing is recorded
+// if they cannot be allocated).
 static void tune_fold(Launcher &L, const TuneKey &k, const uint32_t *rs, const uint32_t *d_rs) {
     const uint64_t n = 1ull << k.log_len;
     uint32_t *in = nullptr, *out = nullptr, *drs = nullptr;
@@ -1723,8 +1753,9 @@ static void tune_fold(Launcher &L, const TuneKey &k, const uint32_t *rs, const u
     L.timing = false;
     int best = 4;
     float best_ms = 1e30f;
-    for (int bps = 1; bps <= 4; ++bps) {
-        L.forced_fold_bps = bps;
+    for (int cand = 0; cand < 8; ++cand) {
+        const int bps = 1 + (cand & 3), choice = bps | ((cand >> 2) << 8);
+        L.forced_fold_bps = choice;
         float ms = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             cudaEventRecord(a, L.stream);
@@ -1735,7 +1766,7 @@ static void tune_fold(Launcher &L, const TuneKey &k, const uint32_t *rs, const u
             cudaEventElapsedTime(&t, a, b);
             if (rep > 0) ms = std::min(ms, t);
         }
-        if (ms < best_ms) { best_ms = ms; best = bps; }
+        if (ms < best_ms) { best_ms = ms; best = choice; }
     }
     L.forced_fold_bps = 0;
     L.timing = timing;
@@ -1764,8 +1795,9 @@ std::string tuned_choices() {
         s += "\n";
     }
     for (auto &kv : g_fold_bps) {
-        std::snprintf(buf, sizeof buf, "fold device %d log_len %u k %u : blocks/SM %d\n", kv.first.device,
-                      kv.first.log_len, kv.first.nvec, kv.second);
+        std::snprintf(buf, sizeof buf, "fold device %d log_len %u k %u : blocks/SM %d outputs/thread %d\n",
+                      kv.first.device, kv.first.log_len, kv.first.nvec, kv.second & 0xFF,
+                      (kv.second & 0x100) ? 4 : 1);
         s += buf;
     }
     return s;
