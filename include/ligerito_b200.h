@@ -169,6 +169,19 @@ void lg_proof_free(lg_proof *proof);
 /* ProofSize::proof_size, src/data_structures.rs:165-194 */
 lg_status lg_proof_size(const lg_proof *proof, uint64_t *bytes);
 
+/* Lockstep batch: `count` polynomials of one config (each `len` words, on
+ * the device or all on the host) proved together on one context, up to 64
+ * per group, every kernel launch covering the whole group (the proof index
+ * is a grid dimension); out[i] is the proof of polys[i], the same bytes
+ * lg_prove gives alone.  Device inputs that are already contiguous
+ * (polys[i] = polys[0] + i * len) are read in place, others are first
+ * copied into one buffer.  A proof whose prover assertion fails gets
+ * out[i] = NULL and the call returns LG_ERR_PROVER_ASSERT; other proofs of
+ * the call are still returned.  (A loop of src/prover.rs:15 over the
+ * polynomials.) */
+lg_status lg_prove_lockstep(lg_ctx *ctx, const lg_config *cfg, const uint32_t *const *polys, uint64_t len,
+                            uint32_t count, int polys_on_device, lg_proof **out);
+
 /* ------------------------------------------------- batched / served proving
  * Many proofs of uneven sizes on one GPU.  A server runs `workers`
  * threads, each with its own context; requests are admitted FIFO when their
@@ -180,6 +193,11 @@ lg_status lg_proof_size(const lg_proof *proof, uint64_t *bytes);
  * call, src/prover.rs:15; these have no counterpart there.) */
 typedef struct lg_server lg_server;
 lg_status lg_server_create(int device, uint64_t hbm_budget_bytes, uint32_t workers, lg_server **out);
+/* A worker that takes a request also takes up to max_batch - 1 queued
+ * requests of the same config and input kind (in queue order, while they
+ * fit the budget) and proves them in lockstep (lg_prove_lockstep).
+ * 1 (the default) proves one request at a time; at most 64. */
+lg_status lg_server_set_max_batch(lg_server *srv, uint32_t max_batch);
 /* copy_input = 1 copies a host polynomial so the caller may free it at
  * once; otherwise (and always for device input) it must stay valid until
  * lg_server_wait returns for this ticket. */

@@ -137,11 +137,13 @@ def _load() -> ctypes.CDLL:
         "lg_fill_splitmix_host": (None, [u64, P, u64]),
         "lg_induce_sumcheck_poly_noalloc": (i32, [P, u32, P, u32, P, u32, P, u32, P, P]),
         "lg_server_create": (i32, [i32, u64, u32, P]),
+        "lg_server_set_max_batch": (i32, [P, u32]),
         "lg_server_submit": (i32, [P, P, P, u64, i32, i32, P]),
         "lg_server_wait": (i32, [P, u64, ctypes.c_int64, P, P, P]),
         "lg_server_stats": (i32, [P, P, P, P]),
         "lg_server_destroy": (None, [P]),
         "lg_prove_batch": (i32, [i32, u32, P, P, P, i32, u32, P]),
+        "lg_prove_lockstep": (i32, [P, P, P, u64, u32, i32, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -593,6 +595,42 @@ def prover(config: ProverConfig, poly, ctx: Optional[Context] = None) -> Finaliz
     return FinalizedLigeritoProof(h)
 
 
+def prove_lockstep(config: ProverConfig, polys, ctx: Optional[Context] = None) -> list:
+    """Many polynomials of one config proved in lockstep on one context
+    (lg_prove_lockstep): every kernel launch covers up to 64 proofs.
+    ``polys``: a 2-D CUDA tensor or host array (one polynomial per row), or
+    a sequence of 1-D ones (all CUDA tensors or all host arrays).  Returns
+    one proof per polynomial, each the bytes ``prover`` gives alone."""
+    ctx = ctx or default_context()
+    c = config.to_c()
+    rows = [polys[i] for i in range(len(polys))]
+    n = len(rows)
+    if n == 0:
+        return []
+    on_dev = 1 if _is_torch(rows[0]) else 0
+    keep = []
+    ptrs = (ctypes.c_void_p * n)()
+    length = None
+    for i, r in enumerate(rows):
+        if on_dev:
+            if not r.is_contiguous():
+                raise ValueError("polynomial rows must be contiguous")
+            ptrs[i], ln = _dev_ptr(r), r.numel()
+        else:
+            a = _u32(r)
+            keep.append(a)
+            ptrs[i], ln = a.ctypes.data, a.size
+        if length is None:
+            length = ln
+        elif ln != length:
+            raise ValueError("lockstep polynomials must all have the config's length")
+    out = (ctypes.c_void_p * n)()
+    st = lib.lg_prove_lockstep(ctx.handle, ctypes.byref(c), ptrs, length, n, on_dev, out)
+    proofs = [FinalizedLigeritoProof(ctypes.c_void_p(out[i])) if out[i] else None for i in range(n)]
+    _check(st, ctx)
+    return proofs
+
+
 def verifier(config, proof, ctx: Optional[Context] = None) -> bool:
     """verifier::<BinaryElem32>(config, proof) (src/verifier.rs:10): the
     reference's bool, or LigeritoPanic where the reference panics."""
@@ -722,10 +760,16 @@ class Server:
     """Continuous-batching proof server (lg_server_*): `workers` concurrent
     contexts on one GPU, FIFO admission under an HBM budget."""
 
-    def __init__(self, device: int = 0, workers: int = 4, hbm_budget_bytes: int = 0):
+    def __init__(self, device: int = 0, workers: int = 4, hbm_budget_bytes: int = 0, max_batch: int = 1):
         self.handle = ctypes.c_void_p()
         _check(lib.lg_server_create(device, hbm_budget_bytes, workers, ctypes.byref(self.handle)))
         self._keep = {}
+        if max_batch != 1:
+            self.set_max_batch(max_batch)
+
+    def set_max_batch(self, max_batch: int) -> None:
+        """Same-config queued requests a worker proves in lockstep (1..64)."""
+        _check(lib.lg_server_set_max_batch(self.handle, max_batch))
 
     def submit(self, config: ProverConfig, poly, copy_input: bool = False) -> int:
         c = config.to_c()

@@ -712,6 +712,332 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
     throw ProverAssert{};  // :198
 }
 
+// ------------------------------------------------------ lockstep batches
+// B proofs of one config in lockstep: each kernel launch of the prover
+// above takes all B proofs at once (the proof index is a grid dimension),
+// proof b in its own slice of every buffer, so that small proofs fill the
+// GPU and the launch and transcript latencies are paid once per batch.
+// The B polynomials are contiguous on the device (proof b at
+// d_polys + b * len); the columns of a commitment are independent, so the
+// B encodings are one matrix of B * n columns.  Each proof is the bytes
+// prove_impl gives alone.
+struct BatchWitness {
+    DBuf E, tree;
+    uint64_t rows = 0;
+    uint32_t cols = 0, B = 0;
+    uint64_t e_stride() const { return rows * cols; }       // words per proof
+    uint64_t t_stride() const { return 8 * (2 * rows - 1); } // words per proof
+    const uint32_t *root() const { return tree.u32() + 8 * (2 * rows - 2); }  // proof 0's
+};
+
+BatchWitness commit_batch(lg_ctx *c, const uint32_t *d_polys, uint32_t log_m, uint32_t n, uint32_t B) {
+    const Code code = get_code(c, log_m);
+    BatchWitness w;
+    w.rows = 4ull << log_m;
+    w.cols = n;
+    w.B = B;
+    w.E = DBuf(c, 4ull * B * w.e_stride());
+    w.tree = DBuf(c, 4ull * B * w.t_stride());
+    {
+        DBuf scaled(c, log_m > 6 ? 4ull * B * n << log_m : 0);
+        rs_encode(c, code, d_polys, log_m, B * n, w.E.u32(), w.rows, scaled.u32());
+    }
+    CK(c, lgk::leaf_hashes(c->L, w.E.u32(), w.rows, n, w.tree.u32(), B, w.e_stride(), w.t_stride()));
+    CK(c, lgk::merkle_upper(c->L, w.tree.u32(), w.rows, B, w.t_stride()));
+    return w;
+}
+
+// open_rows_dev for the B proofs: fs_queries absorbs each proof's `absorb`
+// (8 words, proof b at absorb + b * absorb_stride; nothing when absorb is
+// null) and draws its queries and
+// node list; one gather opens all.  Returns the device copy of the opened
+// rows (proof b at rows + b * stride) and of the queries (nq per proof).
+struct BatchOpened {
+    const uint32_t *rows;
+    uint64_t stride;
+    const uint64_t *q;
+};
+BatchOpened open_rows_batch(lg_ctx *c, Scratch &sc, const BatchWitness &w, lgk::FsState *fs, const uint32_t *absorb,
+                            uint64_t absorb_stride, uint32_t nsq, uint32_t *out, uint64_t out_stride,
+                            const std::vector<lg::Opening *> &ops, uint32_t *mirror) {
+    const uint32_t nq = LG_NUM_QUERIES, B = w.B;
+    uint32_t depth = 0;
+    while ((1ull << depth) < w.rows) ++depth;
+    const uint32_t cap = nq * std::max<uint32_t>(depth, 1);
+    const uint64_t os = ((uint64_t)nq * w.cols + (uint64_t)cap * 8 + 1 + 3) & ~3ull;  // words per proof
+    uint64_t *d_q = static_cast<uint64_t *>(sc.dev(8ull * nq * B));
+    uint64_t *d_nodes = static_cast<uint64_t *>(sc.dev(8ull * cap * B));
+    uint32_t *d_out = static_cast<uint32_t *>(sc.dev(4ull * os * B));
+    uint32_t *d_cnt = d_out + (uint64_t)nq * w.cols + (uint64_t)cap * 8;
+    lgk::FsQueries a;
+    a.src = absorb;
+    a.nwords = absorb ? 8 : 0;
+    a.n = w.rows;
+    a.s = nq;
+    a.q = d_q;
+    a.nodes = d_nodes;
+    a.nodes_cap = cap;
+    a.nnodes = d_cnt;
+    a.nsq = nsq;
+    a.out = out;
+    a.mirror = mirror;
+    lgk::FsStrides fst;
+    fst.src = absorb_stride;
+    fst.out = out_stride;
+    fst.mirror = 8;
+    fst.q = nq;
+    fst.nodes = cap;
+    fst.nnodes = os;
+    CK(c, lgk::fs_queries(c->L, fs, a, B, fst));
+    lgk::GatherStrides gst;
+    gst.E = w.e_stride();
+    gst.q = nq;
+    gst.tree = w.t_stride();
+    gst.nodes = cap;
+    gst.count = os;
+    gst.out = os;
+    CK(c, lgk::gather_opening(c->L, w.E.u32(), w.rows, w.cols, d_q, nq, w.tree.u32(), d_nodes, cap, d_cnt, d_out, B,
+                              gst));
+    const uint32_t *h = sc.download_deferred(d_out, os * B);
+    const uint32_t cols = w.cols;
+    sc.finalizers.push_back([h, nq, cap, cols, os, ops]() {
+        for (size_t b = 0; b < ops.size(); ++b) {
+            const uint32_t *hb = h + b * os;
+            ops[b]->rows.assign_fixed(hb, nq, cols);
+            const uint32_t nr = std::min(hb[(uint64_t)nq * cols + (uint64_t)cap * 8], cap);
+            ops[b]->merkle.assign_fixed(reinterpret_cast<const uint8_t *>(hb + (uint64_t)nq * cols), nr, 32);
+        }
+    });
+    return {d_out, os, d_q};
+}
+
+// induce_dev for the B proofs: rows (nq x 2^nch each, proof b at
+// d_rows + b * rows_stride), queries (nq each), basis out (2^n each), the
+// enforced sums (d_sum + b * sum_stride) and the device challenges (vch,
+// alpha: + b * chal_stride).
+void induce_batch(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *d_rows, uint64_t rows_stride, uint32_t nq,
+                  uint32_t nch, const uint64_t *d_q, uint32_t *d_out, uint32_t *d_sum, uint64_t sum_stride,
+                  const uint32_t *d_vch, const uint32_t *d_alpha, uint64_t chal_stride, uint32_t B) {
+    std::vector<uint32_t> sks = lg::eval_sk_at_vks(1ull << n);
+    const lgk::InducePlan plan = lgk::induce_plan(n, nq);
+    lgk::InduceStrides st;
+    st.rows = rows_stride;
+    st.q = nq;
+    st.S = (uint64_t)nq * std::max<uint32_t>(n, 1);
+    st.apow = 2ull * nq;
+    st.lo = (uint64_t)nq << plan.b;
+    st.hi = (uint64_t)nq << (n - plan.b);
+    st.out = 1ull << n;
+    st.sum = sum_stride;
+    st.rs = chal_stride;
+    st.alpha = chal_stride;
+    uint32_t *d_S = static_cast<uint32_t *>(sc.dev(4ull * st.S * B));
+    uint32_t *d_apow = static_cast<uint32_t *>(sc.dev(4ull * st.apow * B));
+    uint32_t *d_lo = static_cast<uint32_t *>(sc.dev(4ull * st.lo * B));
+    uint32_t *d_hi = static_cast<uint32_t *>(sc.dev(4ull * st.hi * B));
+    CK(c, lgk::induce_setup(c->L, d_rows, 1u << nch, nullptr, d_q, nq, 0, n, sks.data(), d_S, d_apow, d_vch, d_alpha,
+                            B, st));
+    if (plan.needs_zero) CK(c, cudaMemsetAsync(d_out, 0, (4ull << n) * B, c->stream));
+    CK(c, lgk::induce_basis(c->L, plan, d_S, d_apow, n, nq, d_lo, d_hi, d_out, d_sum, B, st));
+}
+
+// partial_eval_dev for the B proofs (inputs in_stride apart, outputs and
+// intermediates packed, challenges rs_stride apart)
+void partial_eval_batch(lg_ctx *c, const uint32_t *d_in, uint64_t in_stride, uint32_t log_len, uint32_t k,
+                        uint32_t *d_out, const uint32_t *d_rs, uint64_t rs_stride, uint32_t B) {
+    DBuf tmp[2];
+    const uint32_t *src = d_in;
+    uint64_t src_stride = in_stride;
+    uint32_t cur = log_len, done = 0, which = 0;
+    while (done < k) {
+        const uint32_t kk = std::min<uint32_t>(6, k - done);
+        uint32_t *dst;
+        if (done + kk == k) dst = d_out;
+        else {
+            tmp[which] = DBuf(c, (4ull << (cur - kk)) * B);
+            dst = tmp[which].u32();
+        }
+        lgk::FoldStrides st;
+        st.in = src_stride;
+        st.out = 1ull << (cur - kk);
+        st.rs = rs_stride;
+        CK(c, lgk::fold_eq(c->L, src, dst, cur, kk, nullptr, d_rs + done, B, st));
+        src = dst;
+        src_stride = st.out;
+        which ^= 1;
+        cur -= kk;
+        done += kk;
+    }
+}
+
+// prove_impl for B proofs of cfg in lockstep.  P[b] receives proof b;
+// bad[b] is set when proof b's prover assertion fails (its P[b] is then
+// incomplete).
+void prove_batch_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_polys, uint64_t len,
+                      uint32_t B, const std::vector<lg::Proof *> &P, std::vector<char> &bad) {
+    if (B == 0 || B > lgk::kMaxTickets || P.size() != B) throw BadConfig{};
+    bad.assign(B, 0);
+    const uint32_t steps = cfg.recursive_steps;
+    uint32_t nrounds = 0;
+    for (uint32_t i = 0; i < steps; ++i) nrounds += cfg.ks[i];
+    const uint32_t ntri = 1 + nrounds + (steps - 1);
+    // per-proof strides (words): challenges, then triples + the fused
+    // steps' ticket
+    const uint64_t CH = (cfg.initial_k + nrounds + 3 * steps + 4 + 3) & ~3u, TR = 4ull * ntri + 4;
+    auto *fs = static_cast<lgk::FsState *>(sc.dev(sizeof(lgk::FsState) * B));
+    uint32_t *chal = static_cast<uint32_t *>(sc.dev(4ull * CH * B));
+    uint32_t *tri = static_cast<uint32_t *>(sc.dev(4ull * TR * B));
+    uint32_t nchal = 0, ntri_used = 0;
+    auto next_chal = [&](uint32_t n) { uint32_t *p = chal + nchal; nchal += n; return p; };
+    auto next_tri = [&]() { return tri + 4 * ntri_used++; };
+    CK(c, cudaMemsetAsync(tri, 0, 4ull * TR * B, c->stream));
+    CK(c, lgk::fs_init(c->L, fs, LG_FS_SEED, B));
+    auto root_later = [&](std::vector<std::vector<uint8_t> *> dst) {
+        uint32_t *mirror = static_cast<uint32_t *>(sc.dev(32ull * B));
+        const uint32_t *h = sc.download_deferred(mirror, 8ull * B);
+        sc.finalizers.push_back([h, dst]() {
+            for (size_t b = 0; b < dst.size(); ++b) {
+                const uint8_t *p = reinterpret_cast<const uint8_t *>(h + 8 * b);
+                dst[b]->assign(p, p + 32);
+            }
+        });
+        return mirror;
+    };
+    auto each = [&](auto get) {
+        std::vector<decltype(get(P[0]))> v;
+        for (auto *p : P) v.push_back(get(p));
+        return v;
+    };
+    auto tail = [&](bool check, uint32_t nsq, uint32_t *out) {
+        lgk::FsTail a;
+        a.fs = fs;
+        a.ticket = tri + 4 * ntri;
+        a.check = check;
+        a.nsq = nsq;
+        a.out = out;
+        return a;
+    };
+    auto rstr = [&](uint32_t fv) {
+        lgk::RoundStrides st;
+        st.f = st.g = 1ull << fv;
+        st.fo = st.go = 1ull << (fv - 1);
+        st.acc = TR;
+        st.r = CH;
+        st.fs = 1;
+        st.ticket = TR;
+        st.out = CH;
+        return st;
+    };
+    const uint32_t nq = LG_NUM_QUERIES;
+
+    for (auto *p : P) {
+        p->recursive_roots.resize(steps);
+        p->recursive.resize(steps - 1);
+    }
+    BatchWitness w0 = commit_batch(c, d_polys, cfg.initial_log_m, 1u << cfg.initial_log_n, B);  // :32-37
+    uint32_t *root_m = root_later(each([](lg::Proof *p) { return &p->initial_root; }));
+    const uint32_t *pe0 = next_chal(cfg.initial_k);
+    {
+        lgk::FsStep a;
+        a.src = w0.root();
+        a.nwords = 8;
+        a.nsq = cfg.initial_k;
+        a.out = const_cast<uint32_t *>(pe0);
+        a.mirror = root_m;
+        lgk::FsStrides st;
+        st.src = w0.t_stride();
+        st.out = CH;
+        st.mirror = 8;
+        CK(c, lgk::fs_step(c->L, fs, a, B, st));  // :48-50
+    }
+    uint32_t fv = cfg.initial_log_m;
+    DBuf f(c, (4ull << fv) * B);
+    partial_eval_batch(c, d_polys, len, cfg.initial_log_m + cfg.initial_log_n, cfg.initial_k, f.u32(), pe0, CH,
+                       B);  // :52-53
+
+    BatchWitness wprev = commit_batch(c, f.u32(), cfg.log_m[0], 1u << cfg.log_n[0], B);  // :55-60
+    root_m = root_later(each([](lg::Proof *p) { return &p->recursive_roots[0]; }));
+    uint32_t *alpha = next_chal(1);
+    BatchOpened op = open_rows_batch(c, sc, w0, fs, wprev.root(), wprev.t_stride(), 1, alpha, CH,
+                                     each([](lg::Proof *p) { return &p->initial; }), root_m);  // :64-76
+    DBuf Bv(c, (4ull << fv) * B);
+    uint32_t *t = next_tri();
+    induce_batch(c, sc, fv, op.rows, op.stride, nq, cfg.initial_k, op.q, Bv.u32(), t + 3, TR, pe0, alpha, CH,
+                 B);  // :78-85
+    w0.E.reset();
+    w0.tree.reset();
+    uint32_t *r = next_chal(1);
+    const lgk::FsTail t0 = tail(true, 1, r);
+    CK(c, lgk::eval013(c->L, f.u32(), Bv.u32(), fv, t, &t0, B, rstr(fv)));
+
+    DBuf f2(c, (4ull << (fv - 1)) * B), B2(c, (4ull << (fv - 1)) * B);
+    for (uint32_t i = 0; i < steps; ++i) {
+        const uint32_t *rs = r;
+        for (uint32_t k = 0; k < cfg.ks[i]; ++k) {  // :97-102
+            t = next_tri();
+            const bool more = k + 1 < cfg.ks[i];
+            uint32_t *rn = more ? next_chal(1) : nullptr;
+            const lgk::FsTail tk = tail(false, more ? 1 : 0, rn);
+            CK(c, lgk::fold_round(c->L, f.u32(), Bv.u32(), fv, 0, f2.u32(), B2.u32(), t, r, &tk, B, rstr(fv)));
+            std::swap(f, f2);
+            std::swap(Bv, B2);
+            fv -= 1;
+            r = rn;
+        }
+        if (i == steps - 1) {  // :104-143
+            // The rest of each transcript runs on the device as well (one
+            // block per proof, all at once): absorb yr, draw the final
+            // queries and their node list, and one gather opens every
+            // proof -- no host round trip inside the batch.
+            const uint64_t ny = 1ull << fv;
+            for (uint64_t off = 0; off < ny; off += 1024) {
+                lgk::FsStep a;
+                a.src = f.u32() + off;
+                a.nwords = (uint32_t)std::min<uint64_t>(1024, ny - off);
+                lgk::FsStrides st;
+                st.src = ny;
+                CK(c, lgk::fs_step(c->L, fs, a, B, st));
+            }
+            open_rows_batch(c, sc, wprev, fs, nullptr, 0, 0, nullptr, 0,
+                            each([](lg::Proof *p) { return &p->final_; }), nullptr);
+            // (f is freed when this returns: its copy is queued now)
+            const uint32_t *hy = sc.download_later(f.u32(), ny * B);
+            const lgk::FsState *hs = sc.download_deferred(fs, B);
+            const uint32_t *ht = sc.download_deferred(tri, TR * B);
+            std::vector<char> *flags = &bad;
+            sc.finalizers.push_back([hy, hs, ht, ny, ntri, TR, P, flags]() {
+                for (size_t b = 0; b < P.size(); ++b) {
+                    lg::Proof &pb = *P[b];
+                    pb.yr.assign(hy + b * ny, hy + (b + 1) * ny);
+                    for (uint32_t j = 0; j < ntri; ++j) {
+                        const uint32_t *x = ht + b * TR + 4 * j;
+                        pb.transcript.push_back({x[0], x[1], x[2]});
+                    }
+                    (*flags)[b] = hs[b].err != 0;  // a prover assertion failed on the device
+                }
+            });
+            return;
+        }
+        BatchWitness wn = commit_batch(c, f.u32(), cfg.log_m[i + 1], 1u << cfg.log_n[i + 1], B);  // :145-155
+        const uint32_t ip1 = i + 1, ii = i;
+        root_m = root_later(each([ip1](lg::Proof *p) { return &p->recursive_roots[ip1]; }));
+        uint32_t *al = next_chal(1);
+        BatchOpened o = open_rows_batch(c, sc, wprev, fs, wn.root(), wn.t_stride(), 1, al, CH,
+                                        each([ii](lg::Proof *p) { return &p->recursive[ii]; }), root_m);  // :156-172
+        DBuf bi(c, (4ull << fv) * B);
+        t = next_tri();
+        induce_batch(c, sc, fv, o.rows, o.stride, nq, cfg.ks[i], o.q, bi.u32(), t + 3, TR, rs, al, CH, B);
+        uint32_t *beta = next_chal(2);
+        const lgk::FsTail ti = tail(true, 2, beta);
+        CK(c, lgk::eval013(c->L, f.u32(), bi.u32(), fv, t, &ti, B, rstr(fv)));
+        r = beta + 1;
+        lgk::RoundStrides ax = rstr(fv);
+        CK(c, lgk::axpy(c->L, Bv.u32(), bi.u32(), fv, 0, beta, B, ax));  // glue
+        wprev = std::move(wn);
+    }
+    throw ProverAssert{};  // :198
+}
+
 // ---------------------------------------------------------------- verifier
 struct Quad { uint32_t a, b, c; };  // QuadraticPoly, src/sumcheck.rs:38-65
 Quad quad_from_evals(uint32_t at0, uint32_t at1, uint32_t atx) {  // :67-81, x = 3
@@ -1363,6 +1689,64 @@ lg_status lg_prove(lg_ctx *c, const lg_config *cfg, const uint32_t *poly, uint64
     if (st != LG_OK) { delete res; return st; }
     *out = res;
     return LG_OK;
+}
+
+lg_status lg_prove_lockstep(lg_ctx *c, const lg_config *cfg, const uint32_t *const *polys, uint64_t len,
+                            uint32_t count, int on_device, lg_proof **out) {
+    if (!c || !cfg || !polys || !out) return LG_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i) {
+        out[i] = nullptr;
+        if (!polys[i]) return LG_ERR_INVALID_ARGUMENT;
+    }
+    lg_status st = lg::config_check(*cfg, len);
+    if (st != LG_OK) return st;
+    lg_status first = LG_OK;
+    for (uint32_t s0 = 0; s0 < count; s0 += lgk::kMaxTickets) {
+        const uint32_t B = std::min<uint32_t>(lgk::kMaxTickets, count - s0);
+        std::vector<lg_proof *> res(B, nullptr);
+        std::vector<char> bad;
+        for (auto &r : res) {
+            r = new (std::nothrow) lg_proof;
+            if (!r) {
+                for (auto *x : res) delete x;
+                return first != LG_OK ? first : LG_ERR_OUT_OF_MEMORY;
+            }
+        }
+        st = guarded(c, [&] {
+            CK(c, cudaSetDevice(c->device));
+            Scratch sc(c);
+            // the inputs as one contiguous run, copied together unless
+            // they already are
+            bool contiguous = on_device != 0;
+            for (uint32_t b = 1; b < B && contiguous; ++b) contiguous = polys[s0 + b] == polys[s0] + b * len;
+            DBuf in;
+            const uint32_t *d = polys[s0];
+            if (!contiguous) {
+                in = DBuf(c, 4 * len * B);
+                for (uint32_t b = 0; b < B; ++b)
+                    CK(c, cudaMemcpyAsync(in.u32() + b * len, polys[s0 + b], 4 * len,
+                                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+                d = in.u32();
+            }
+            std::vector<lg::Proof *> P(B);
+            for (uint32_t b = 0; b < B; ++b) P[b] = &res[b]->p;
+            prove_batch_impl(c, sc, *cfg, d, len, B, P, bad);
+            sc.finish();
+        });
+        for (uint32_t b = 0; b < B; ++b) {
+            if (st == LG_OK && !bad[b]) {
+                out[s0 + b] = res[b];
+            } else {
+                delete res[b];
+                if (st == LG_OK) {
+                    c->err = "prover assertion failed";
+                    if (first == LG_OK) first = LG_ERR_PROVER_ASSERT;
+                }
+            }
+        }
+        if (st != LG_OK && first == LG_OK) first = st;
+    }
+    return first;
 }
 
 lg_status lg_verify(lg_ctx *c, const lg_config *cfg, const lg_proof *proof, int *accepted) {

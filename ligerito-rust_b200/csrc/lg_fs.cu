@@ -28,6 +28,7 @@ using lgd::pdl_begin;
 
 __global__ void k_fs_init(FsState *g, uint32_t seed) {
     pdl_begin();
+    g += blockIdx.x;  // lockstep batch: one block per proof
     __shared__ FsState S;
     if (threadIdx.x == 0) {
         const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
@@ -43,8 +44,15 @@ __global__ void k_fs_init(FsState *g, uint32_t seed) {
     store_state(S, g);
 }
 
-__global__ void k_fs_step(FsState *g, FsStep a) {
+__global__ void k_fs_step(FsState *g, FsStep a, FsStrides st) {
     pdl_begin();
+    {
+        const uint32_t b = blockIdx.x;  // lockstep batch: one block per proof
+        g += b;
+        a.src += b * st.src;
+        if (a.out) a.out += b * st.out;
+        if (a.mirror) a.mirror += b * st.mirror;
+    }
     __shared__ FsState S;
     __shared__ Batch B;
     __shared__ uint32_t stage[32];
@@ -117,8 +125,18 @@ __device__ void fs_chain_block(const FsState &S, Batch &B, uint32_t cnt, uint32_
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a) {
+__global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a, FsStrides st) {
     pdl_begin();
+    {
+        const uint32_t b = blockIdx.x;  // lockstep batch: one block per proof
+        g += b;
+        if (a.src) a.src += b * st.src;
+        if (a.out) a.out += b * st.out;
+        if (a.mirror) a.mirror += b * st.mirror;
+        a.q += b * st.q;
+        a.nodes += b * st.nodes;
+        a.nnodes += b * st.nnodes;
+    }
     __shared__ FsState S;
     __shared__ Batch B;
     __shared__ uint64_t acc[kQBlock];
@@ -290,21 +308,25 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a)
 
 }  // namespace
 
-cudaError_t fs_init(Launcher &L, FsState *d, uint32_t seed) {
-    LGK_LAUNCH(L, "fs_init", launch_k(k_fs_init, 1, 32, 0, L.stream, d, seed));
+cudaError_t fs_init(Launcher &L, FsState *d, uint32_t seed, uint32_t B) {
+    if (B == 0 || B > 65535) return cudaErrorInvalidValue;
+    LGK_LAUNCH(L, "fs_init", launch_k(k_fs_init, B, 32, 0, L.stream, d, seed));
     return cudaGetLastError();
 }
 
-cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a) {
-    if (a.nwords > 1024 || a.nsq > 256 || (a.check && (!a.src || a.nwords < 3))) return cudaErrorInvalidValue;
-    LGK_LAUNCH(L, "fs_step", launch_k(k_fs_step, 1, 32, 0, L.stream, d, a));
-    return cudaGetLastError();
-}
-
-cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a) {
-    if (a.s == 0 || a.s > kQBlock || a.n == 0 || (a.n & (a.n - 1)) || a.nwords > 1024 || a.nsq > kQBlock)
+cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a, uint32_t B, const FsStrides &st) {
+    if (a.nwords > 1024 || (a.nwords && !a.src) || a.nsq > 256 || (a.nsq && !a.out) ||
+        (a.check && (!a.src || a.nwords < 3)) || B == 0 || B > 65535)
         return cudaErrorInvalidValue;
-    LGK_LAUNCH(L, "fs_queries", launch_k(k_fs_queries, 1, kQBlock, 0, L.stream, d, a));
+    LGK_LAUNCH(L, "fs_step", launch_k(k_fs_step, B, 32, 0, L.stream, d, a, st));
+    return cudaGetLastError();
+}
+
+cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a, uint32_t B, const FsStrides &st) {
+    if (a.s == 0 || a.s > kQBlock || a.n == 0 || (a.n & (a.n - 1)) || a.nwords > 1024 || (a.nwords && !a.src) ||
+        a.nsq > kQBlock || (a.nsq && !a.out) || !a.q || !a.nodes || !a.nnodes || B == 0 || B > 65535)
+        return cudaErrorInvalidValue;
+    LGK_LAUNCH(L, "fs_queries", launch_k(k_fs_queries, B, kQBlock, 0, L.stream, d, a, st));
     return cudaGetLastError();
 }
 

@@ -700,8 +700,10 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
 // Leaf = the row's n words as LE bytes, one BLAKE3 chunk (n <= 256):
 // blocks of 16 words, CHUNK_START on the first, CHUNK_END|ROOT on the last.
 __global__ void k_leaf_hash(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
-                            uint32_t *__restrict__ out, uint32_t one) {
+                            uint32_t *__restrict__ out, uint32_t one, uint64_t e_stride, uint64_t out_stride) {
     pdl_begin();
+    E += blockIdx.y * e_stride;  // lockstep batch: proof blockIdx.y
+    out += blockIdx.y * out_stride;
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const uint32_t nb = (ncols + 15) / 16;
@@ -765,10 +767,13 @@ cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint3
     return cudaGetLastError();
 }
 
-cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out) {
-    const unsigned blocks = (unsigned)((rows + 127) / 128);
-    L.note((double)rows * (4.0 * ncols + 32.0), 0, (double)rows * ((ncols + 15) / 16));
-    LGK_LAUNCH(L, "leaf_hash", launch_k(k_leaf_hash, blocks, 128, 0, L.stream, E, rows, ncols, out, 1u));
+cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out, uint32_t B,
+                        uint64_t e_stride, uint64_t out_stride) {
+    if (B == 0 || B > 65535) return cudaErrorInvalidValue;
+    const dim3 blocks((unsigned)((rows + 127) / 128), B);
+    L.note((double)B * rows * (4.0 * ncols + 32.0), 0, (double)B * rows * ((ncols + 15) / 16));
+    LGK_LAUNCH(L, "leaf_hash", launch_k(k_leaf_hash, blocks, 128, 0, L.stream, E, rows, ncols, out, 1u, e_stride,
+                                        out_stride));
     return cudaGetLastError();
 }
 
@@ -805,8 +810,9 @@ __device__ __forceinline__ void hash_pair(const uint32_t (&l)[8], const uint32_t
 }
 
 __global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
-                                                        uint32_t one) {
+                                                        uint32_t one, uint64_t tree_stride) {
     pdl_begin();
+    tree += blockIdx.y * tree_stride;  // lockstep batch: proof blockIdx.y
     const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (8 * t >= n_in) return;
     const uint64_t off1 = in_off + n_in, off2 = off1 + n_in / 2, off3 = off2 + n_in / 4;
@@ -899,8 +905,10 @@ __device__ __forceinline__ void narrow_climb(uint32_t *__restrict__ tree, uint64
 }
 
 __global__ void __launch_bounds__(256) k_merkle_narrow(uint32_t *__restrict__ tree, uint64_t in_off, uint64_t n_in,
-                                                       uint32_t *ticket, uint32_t one) {
+                                                       uint32_t *ticket, uint32_t one, uint64_t tree_stride) {
     pdl_begin();
+    tree += blockIdx.y * tree_stride;  // lockstep batch: proof blockIdx.y, its own ticket
+    ticket += blockIdx.y;
     // layers in shared memory word-major (word j of node i at [j * stride +
     // i]): a thread reads its two children's word j as one 8-byte load
     __shared__ __align__(16) uint32_t buf_a[8 * (kNarrowNodes / 2)];
@@ -921,8 +929,9 @@ __global__ void __launch_bounds__(256) k_merkle_narrow(uint32_t *__restrict__ tr
     narrow_climb(tree, off, n, 0, nb, buf_a, buf_b, one);
 }
 
-cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
-    if (num_leaves == 0 || (num_leaves & (num_leaves - 1)) || !L.tickets) return cudaErrorInvalidValue;
+cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves, uint32_t B, uint64_t tree_stride) {
+    if (num_leaves == 0 || (num_leaves & (num_leaves - 1)) || !L.tickets || B == 0 || B > kMaxTickets)
+        return cudaErrorInvalidValue;
     uint64_t off = 0, n = num_leaves;
     // Three layers per launch with a thread per 8 nodes while a layer has
     // more than 2^18 nodes (every lane does full work); from a layer of
@@ -931,16 +940,16 @@ cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
         cudaError_t e;
         if (n > kNarrowMax) {
             const uint64_t threads = n / 8;
-            L.note(32.0 * (n + n / 2 + n / 4 + n / 8), (double)0, (double)(n / 2 + n / 4 + n / 8));
-            LGK_LAUNCH(L, "merkle_thread3", launch_k(k_merkle_thread3, (unsigned)((threads + 127) / 128), 128, 0,
-                                                     L.stream, tree, off, n, 1u));
+            L.note(32.0 * B * (n + n / 2 + n / 4 + n / 8), (double)0, (double)B * (n / 2 + n / 4 + n / 8));
+            LGK_LAUNCH(L, "merkle_thread3", launch_k(k_merkle_thread3, dim3((unsigned)((threads + 127) / 128), B), 128,
+                                                     0, L.stream, tree, off, n, 1u, tree_stride));
             e = cudaGetLastError();
             for (int l = 0; l < 3; ++l) { off += n; n /= 2; }
         } else {
             const uint64_t per = std::min<uint64_t>(n, kNarrowNodes);
-            L.note(32.0 * (2 * n - 1), 0, (double)(n - 1));
-            LGK_LAUNCH(L, "merkle_narrow", launch_k(k_merkle_narrow, (unsigned)(n / per), 256, 0, L.stream, tree, off,
-                                                    n, L.tickets, 1u));
+            L.note(32.0 * B * (2 * n - 1), 0, (double)B * (n - 1));
+            LGK_LAUNCH(L, "merkle_narrow", launch_k(k_merkle_narrow, dim3((unsigned)(n / per), B), 256, 0, L.stream,
+                                                    tree, off, n, L.tickets, 1u, tree_stride));
             e = cudaGetLastError();
             n = 1;
         }
@@ -956,8 +965,15 @@ cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves) {
 __global__ void k_gather_opening(const uint32_t *__restrict__ E, uint64_t rows, uint32_t ncols,
                                  const uint64_t *__restrict__ q, uint32_t nq, const uint32_t *__restrict__ tree,
                                  const uint64_t *__restrict__ node_idx, uint32_t count, const uint32_t *d_count,
-                                 uint32_t *__restrict__ out) {
+                                 uint32_t *__restrict__ out, GatherStrides st) {
     pdl_begin();
+    const uint32_t b = blockIdx.y;  // lockstep batch: proof b
+    E += b * st.E;
+    q += b * st.q;
+    tree += b * st.tree;
+    node_idx += b * st.nodes;
+    if (d_count) d_count += b * st.count;
+    out += b * st.out;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, nrow = nq * ncols;
     if (t < nrow) {
         const uint32_t k = t / ncols, j = t % ncols;
@@ -971,13 +987,14 @@ __global__ void k_gather_opening(const uint32_t *__restrict__ E, uint64_t rows, 
 }
 cudaError_t gather_opening(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, const uint64_t *d_queries,
                            uint32_t nq, const uint32_t *tree, const uint64_t *d_node_index, uint32_t count,
-                           const uint32_t *d_count, uint32_t *out) {
+                           const uint32_t *d_count, uint32_t *out, uint32_t B, const GatherStrides &st) {
     const uint64_t total = (uint64_t)nq * ncols + 8ull * count;
     if (total == 0) return cudaSuccess;
-    if (total > 0xFFFFFFFFull) return cudaErrorInvalidValue;
-    L.note(8.0 * total, 0);
-    LGK_LAUNCH(L, "gather_opening", launch_k(k_gather_opening, (unsigned)((total + 255) / 256), 256, 0, L.stream, E,
-                                             rows, ncols, d_queries, nq, tree, d_node_index, count, d_count, out));
+    if (total > 0xFFFFFFFFull || B == 0 || B > 65535) return cudaErrorInvalidValue;
+    L.note(8.0 * B * total, 0);
+    LGK_LAUNCH(L, "gather_opening", launch_k(k_gather_opening, dim3((unsigned)((total + 255) / 256), B), 256, 0,
+                                             L.stream, E, rows, ncols, d_queries, nq, tree, d_node_index, count,
+                                             d_count, out, st));
     return cudaGetLastError();
 }
 
@@ -1006,8 +1023,11 @@ struct Rs6 { uint32_t v[6]; };
 
 template <int KH, int KL, int V>
 __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
-                                                 uint64_t M, Rs6 rs, const uint32_t *d_rs) {
+                                                 uint64_t M, Rs6 rs, const uint32_t *d_rs, FoldStrides st) {
     pdl_begin();
+    in += blockIdx.y * st.in;  // lockstep batch: proof blockIdx.y
+    out += blockIdx.y * st.out;
+    if (d_rs) d_rs += blockIdx.y * st.rs;
     constexpr int NH = 1 << KH, NL = 1 << KL;
     __shared__ __align__(512) uint32_t tabs[NH + NL][kTabWords];  // EL tables, then EH
     __shared__ uint32_t r[KH + KL];
@@ -1069,8 +1089,8 @@ static bool tuned_fold(const TuneKey &k, int *bps);
 static void tune_fold(Launcher &L, const TuneKey &k, const uint32_t *rs, const uint32_t *d_rs);
 
 cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
-                    const uint32_t *rs, const uint32_t *d_rs) {
-    if (k < 1 || k > 6 || k > log_len || (!rs && !d_rs)) return cudaErrorInvalidValue;
+                    const uint32_t *rs, const uint32_t *d_rs, uint32_t B, const FoldStrides &st) {
+    if (k < 1 || k > 6 || k > log_len || (!rs && !d_rs) || B == 0 || B > 65535) return cudaErrorInvalidValue;
     Rs6 c{};
     if (!d_rs)
         for (uint32_t j = 0; j < k; ++j) c.v[j] = rs[j];
@@ -1092,16 +1112,16 @@ cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log
     const int bps = choice & 0xFF;
     const bool vec4 = (choice & 0x100) && M % 4 == 0 && (uintptr_t)in % 16 == 0 && (uintptr_t)out % 16 == 0;
     const uint64_t groups = vec4 ? M / 4 : M;
-    const unsigned blocks =
-        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * (uint64_t)bps));
-    L.note(4.0 * (M << k) + 4.0 * M, (double)M * ((1u << k) + (kh ? (1u << kh) : 0)));
+    const dim3 blocks(
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, 148ull * (uint64_t)bps)), B);
+    L.note(B * (4.0 * (M << k) + 4.0 * M), (double)B * M * ((1u << k) + (kh ? (1u << kh) : 0)));
     switch (2 * k + (vec4 ? 1 : 0)) {
 #define LGK_CASE(kk)                                                                                          \
     case 2 * kk:                                                                                              \
-        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2, 1>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); \
+        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2, 1>, blocks, 256, 0, L.stream, in, out, M, c, d_rs, st)); \
         break;                                                                                                \
     case 2 * kk + 1:                                                                                          \
-        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2, 4>, blocks, 256, 0, L.stream, in, out, M, c, d_rs)); \
+        LGK_LAUNCH(L, "fold_eq", launch_k(k_fold_eq<kk / 2, kk - kk / 2, 4>, blocks, 256, 0, L.stream, in, out, M, c, d_rs, st)); \
         break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(3) LGK_CASE(4) LGK_CASE(5) LGK_CASE(6)
 #undef LGK_CASE
@@ -1130,9 +1150,24 @@ __device__ __forceinline__ void block_xor3(uint32_t s0, uint32_t s1, uint32_t s2
 __device__ __forceinline__ uint32_t at3(uint32_t lo, uint32_t hi) { return gf_mulx(hi ^ lo) ^ hi; }
 
 // eval_013_product (src/multilinear_poly.rs:90-131)
+// the FS tail of proof b of a lockstep batch
+__device__ __forceinline__ FsTail tail_for(FsTail t, const RoundStrides &st, uint32_t b) {
+    if (t.fs) {
+        t.fs += b * st.fs;
+        t.ticket += b * st.ticket;
+        if (t.out) t.out += b * st.out;
+    }
+    return t;
+}
+
 __global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__restrict__ g, uint64_t half,
-                          uint32_t *acc3, FsTail tail) {
+                          uint32_t *acc3, FsTail tail, RoundStrides st) {
     pdl_begin();
+    const uint32_t b = blockIdx.y;  // lockstep batch: proof b
+    f += b * st.f;
+    g += b * st.g;
+    acc3 += b * st.acc;
+    tail = tail_for(tail, st, b);
     uint32_t s0 = 0, s1 = 0, s2 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t f0 = f[i], f1 = f[half + i], g0 = g[i], g1 = g[half + i];
@@ -1144,12 +1179,13 @@ __global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__rest
     if (tail.fs) fsd::fs_tail_block(tail, acc3);
 }
 cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t log_len, uint32_t *acc3,
-                    const FsTail *tail) {
+                    const FsTail *tail, uint32_t B, const RoundStrides &st) {
+    if (B == 0 || B > 65535) return cudaErrorInvalidValue;
     const uint64_t half = 1ull << (log_len - 1);
-    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((half + 255) / 256, 148ull * 4));
+    const dim3 blocks((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((half + 255) / 256, 148ull * 4)), B);
     const FsTail t = tail ? *tail : FsTail{};
-    L.note(16.0 * half, 3.0 * half);
-    LGK_LAUNCH(L, "eval013", launch_k(k_eval013, blocks, 256, 0, L.stream, f, g, half, acc3, t));
+    L.note(16.0 * B * half, 3.0 * B * half);
+    LGK_LAUNCH(L, "eval013", launch_k(k_eval013, blocks, 256, 0, L.stream, f, g, half, acc3, t, st));
     return cudaGetLastError();
 }
 
@@ -1159,8 +1195,18 @@ cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t 
 __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__ f, const uint32_t *__restrict__ B,
                                                     uint64_t quarter, uint32_t r, const uint32_t *d_r,
                                                     uint32_t *__restrict__ fo, uint32_t *__restrict__ Bo,
-                                                    uint32_t *acc3, FsTail tail) {
+                                                    uint32_t *acc3, FsTail tail, RoundStrides st) {
     pdl_begin();
+    {
+        const uint32_t b = blockIdx.y;  // lockstep batch: proof b
+        f += b * st.f;
+        B += b * st.g;
+        fo += b * st.fo;
+        Bo += b * st.go;
+        acc3 += b * st.acc;
+        if (d_r) d_r += b * st.r;
+        tail = tail_for(tail, st, b);
+    }
     __shared__ __align__(128) uint32_t T[kTabWords];
     if (threadIdx.x < 32) tab_build_warp(T, d_r ? *d_r : r, threadIdx.x);
     __syncthreads();
@@ -1181,20 +1227,24 @@ __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__
     if (tail.fs) fsd::fs_tail_block(tail, acc3);
 }
 cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32_t log_len, uint32_t r,
-                       uint32_t *fo, uint32_t *Bo, uint32_t *acc3, const uint32_t *d_r, const FsTail *tail) {
-    if (log_len < 2) return cudaErrorInvalidValue;
+                       uint32_t *fo, uint32_t *Bo, uint32_t *acc3, const uint32_t *d_r, const FsTail *tail,
+                       uint32_t NB, const RoundStrides &st) {
+    if (log_len < 2 || NB == 0 || NB > 65535) return cudaErrorInvalidValue;
     const uint64_t quarter = 1ull << (log_len - 2);
-    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((quarter + 255) / 256, 148ull * 4));
-    L.note(48.0 * quarter, 7.0 * quarter);
+    const dim3 blocks((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((quarter + 255) / 256, 148ull * 4)), NB);
+    L.note(48.0 * NB * quarter, 7.0 * NB * quarter);
     LGK_LAUNCH(L, "fold_round", launch_k(k_fold_round, blocks, 256, 0, L.stream, f, B, quarter, r, d_r, fo, Bo, acc3,
-                                                                                tail ? *tail : FsTail{}));
+                                         tail ? *tail : FsTail{}, st));
     return cudaGetLastError();
 }
 
 // glue (src/ligerito.rs:59-67) folded into the running basis sum
 __global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi, uint64_t n, uint32_t beta,
-                       const uint32_t *d_beta) {
+                       const uint32_t *d_beta, RoundStrides st) {
     pdl_begin();
+    B += blockIdx.y * st.f;  // lockstep batch: proof blockIdx.y
+    bi += blockIdx.y * st.g;
+    if (d_beta) d_beta += blockIdx.y * st.r;
     __shared__ __align__(128) uint32_t T[kTabWords];
     if (threadIdx.x < 32) tab_build_warp(T, d_beta ? *d_beta : beta, threadIdx.x);
     __syncthreads();
@@ -1202,11 +1252,12 @@ __global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi
         B[i] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(T), 0, 0, bi[i]);
 }
 cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta,
-                 const uint32_t *d_beta) {
+                 const uint32_t *d_beta, uint32_t NB, const RoundStrides &st) {
+    if (NB == 0 || NB > 65535) return cudaErrorInvalidValue;
     const uint64_t n = 1ull << log_len;
-    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 4));
-    L.note(12.0 * n, (double)n);
-    LGK_LAUNCH(L, "axpy", launch_k(k_axpy, blocks, 256, 0, L.stream, B, bi, n, beta, d_beta));
+    const dim3 blocks((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 4)), NB);
+    L.note(12.0 * NB * n, (double)NB * n);
+    LGK_LAUNCH(L, "axpy", launch_k(k_axpy, blocks, 256, 0, L.stream, B, bi, n, beta, d_beta, st));
     return cudaGetLastError();
 }
 
@@ -1244,8 +1295,17 @@ __global__ void __launch_bounds__(128) k_induce_setup(const uint32_t *__restrict
                                                       const uint64_t *__restrict__ q, uint32_t nq, uint32_t alpha,
                                                       uint32_t n, InduceSetupArgs args, uint32_t *__restrict__ S,
                                                       uint32_t *__restrict__ apow, const uint32_t *d_rs, uint32_t nch,
-                                                      const uint32_t *d_alpha) {
+                                                      const uint32_t *d_alpha, InduceStrides st) {
     pdl_begin();
+    {
+        const uint32_t b = blockIdx.y;  // lockstep batch: proof b
+        rows += b * st.rows;
+        q += b * st.q;
+        S += b * st.S;
+        apow += b * st.apow;
+        if (d_rs) d_rs += b * st.rs;
+        if (d_alpha) d_alpha += b * st.alpha;
+    }
     // gr: the Lagrange basis of the challenges (from the device when given)
     __shared__ uint32_t gr[256];
     for (uint32_t j = threadIdx.x; j < glen; j += blockDim.x) gr[j] = d_rs ? lagrange_at(d_rs, nch, j) : args.gr[j];
@@ -1279,16 +1339,18 @@ __global__ void __launch_bounds__(128) k_induce_setup(const uint32_t *__restrict
 
 cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
                          const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
-                         uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs, const uint32_t *d_alpha) {
-    if (glen > 256 || n > 32 || nq == 0 || nq > 65536 || (glen & (glen - 1)) || (!gr && !d_rs))
+                         uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs, const uint32_t *d_alpha, uint32_t B,
+                         const InduceStrides &st) {
+    if (glen > 256 || n > 32 || nq == 0 || nq > 65536 || (glen & (glen - 1)) || (!gr && !d_rs) || B == 0 ||
+        B > 65535)
         return cudaErrorInvalidValue;
     InduceSetupArgs args{};
     if (!d_rs)
         for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
     for (uint32_t i = 0; i + 1 < n && i < 32; ++i) args.sks[i] = sks[i];
-    L.note(4.0 * nq * (glen + n + 2), (double)nq * (glen + 2 * n + 20));
-    LGK_LAUNCH(L, "induce_setup", launch_k(k_induce_setup, (nq + 3) / 4, 128, 0, L.stream, d_rows, glen, d_q, nq,
-                                           alpha, n, args, d_S, d_apow, d_rs, ilog2u(glen), d_alpha));
+    L.note(4.0 * B * nq * (glen + n + 2), (double)B * nq * (glen + 2 * n + 20));
+    LGK_LAUNCH(L, "induce_setup", launch_k(k_induce_setup, dim3((nq + 3) / 4, B), 128, 0, L.stream, d_rows, glen, d_q,
+                                           nq, alpha, n, args, d_S, d_apow, d_rs, ilog2u(glen), d_alpha, st));
     return cudaGetLastError();
 }
 
@@ -1301,8 +1363,16 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
 // larger ones double in place in global memory.
 __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__restrict__ apow, uint32_t n,
                               uint32_t b, uint32_t nq, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi,
-                              uint32_t *sum_out, int in_smem) {
+                              uint32_t *sum_out, int in_smem, InduceStrides st) {
     pdl_begin();
+    {
+        const uint32_t pb = blockIdx.y;  // lockstep batch: proof pb
+        S += pb * st.S;
+        apow += pb * st.apow;
+        lo += pb * st.lo;
+        hi += pb * st.hi;
+        sum_out += pb * st.sum;
+    }
     extern __shared__ uint32_t sbuf[];  // Lo then Hi, when in_smem
     __shared__ uint32_t Ss[32];          // the query's subspace values, read once
     const uint32_t k = blockIdx.x, nlo = 1u << b, nhi = 1u << (n - b);
@@ -1340,8 +1410,11 @@ __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__
 template <int ACC>  // ACC = max(1, 2^b / 32) words per lane
 __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
                                                      uint32_t n, uint32_t b, uint32_t nq, uint32_t qs,
-                                                     uint32_t *__restrict__ out, int atomic_out) {
+                                                     uint32_t *__restrict__ out, int atomic_out, InduceStrides st) {
     pdl_begin();
+    lo += blockIdx.z * st.lo;  // lockstep batch: proof blockIdx.z
+    hi += blockIdx.z * st.hi;
+    out += blockIdx.z * st.out;
     __shared__ __align__(128) uint32_t tabs[8][kTabWords];
     __shared__ uint32_t red[32 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -1394,21 +1467,23 @@ __global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict_
 }
 
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
-                         uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum) {
+                         uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum,
+                         uint32_t B, const InduceStrides &st) {
+    if (B == 0 || B > 65535) return cudaErrorInvalidValue;
     const double vec = (double)nq * ((1ull << p.b) + (1ull << (n - p.b)));  // Lo and Hi words
-    L.note(4.0 * vec, vec);
+    L.note(4.0 * B * vec, B * vec);
     const size_t words = (1ull << p.b) + (1ull << (n - p.b));
     const int in_smem = words <= 12288;  // 48 KB: no opt-in needed
-    LGK_LAUNCH(L, "induce_prep", launch_k(k_induce_prep, nq, 256, in_smem ? 4 * words : 0, L.stream, d_S, d_apow, n,
-                                          p.b, nq, d_lo, d_hi, d_sum, in_smem));
+    LGK_LAUNCH(L, "induce_prep", launch_k(k_induce_prep, dim3(nq, B), 256, in_smem ? 4 * words : 0, L.stream, d_S,
+                                          d_apow, n, p.b, nq, d_lo, d_hi, d_sum, in_smem, st));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 grid(1u << (n - p.b), p.qsplit);
+    dim3 grid(1u << (n - p.b), p.qsplit, B);
     const int ao = p.qsplit > 1;
-    L.note(4.0 * (vec + (1ull << n)), (double)nq * (1ull << n));
+    L.note(4.0 * B * (vec + (1ull << n)), (double)B * nq * (1ull << n));
     switch (std::max<uint32_t>(1, (1u << p.b) / 32)) {
 #define LGK_CASE(a) \
-    case a: LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main<a>, grid, 256, 0, L.stream, d_lo, d_hi, n, p.b, nq, p.qsplit, out, ao)); break;
+    case a: LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main<a>, grid, 256, 0, L.stream, d_lo, d_hi, n, p.b, nq, p.qsplit, out, ao, st)); break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(4) LGK_CASE(8) LGK_CASE(16) LGK_CASE(32)
 #undef LGK_CASE
         default: return cudaErrorInvalidValue;

@@ -163,8 +163,15 @@ cudaError_t fft_vectors(Launcher &L, uint32_t *data, const uint32_t *tw, uint32_
                         const FftSrc *src = nullptr);
 
 // --- Merkle (src/merkle_tree.rs:4-60, leaves src/ligero.rs:53-68) --------
+// Lockstep batches: several launchers take B proofs of one config at once,
+// proof b in its own slice of each buffer (buffer + b * that buffer's
+// stride, in elements), the proof index a grid dimension.  B = 1 with zero
+// strides is a single proof.
+constexpr uint32_t kMaxTickets = 64;  // Launcher::tickets words: the largest batch
+
 // Leaf hash of every row of a column-major matrix (rows x ncols u32).
-cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out);
+cudaError_t leaf_hashes(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, uint32_t *out,
+                        uint32_t B = 1, uint64_t e_stride = 0, uint64_t out_stride = 0);
 // BLAKE3 blocks b0 .. b0+nb-1 (columns 16b .. 16b+15 each) of every leaf:
 // chains from the value in out (the IV for b0 = 0) and leaves the chaining
 // value there, the leaf hash after the last block.  Calls cover the blocks
@@ -173,36 +180,47 @@ cudaError_t leaf_hash_block(Launcher &L, const uint32_t *E, uint64_t rows, uint3
                             uint32_t nb, uint32_t *out);
 // All upper layers from the leaf layer at tree[0]; tree as 8-word nodes.
 // Needs the Launcher's tickets.
-cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves);
+cudaError_t merkle_upper(Launcher &L, uint32_t *tree, uint64_t num_leaves, uint32_t B = 1,
+                         uint64_t tree_stride = 0);
 
 // --- gathers for openings (src/ligero.rs:40-51, src/merkle_tree.rs:98) ---
 // out = the nq opened rows (nq x ncols words), then count Merkle nodes (8
 // words each; min(count, *d_count) of them when d_count is given)
+struct GatherStrides { uint64_t E = 0, q = 0, tree = 0, nodes = 0, count = 0, out = 0; };
 cudaError_t gather_opening(Launcher &L, const uint32_t *E, uint64_t rows, uint32_t ncols, const uint64_t *d_queries,
                            uint32_t nq, const uint32_t *tree, const uint64_t *d_node_index, uint32_t count,
-                           const uint32_t *d_count, uint32_t *out);
+                           const uint32_t *d_count, uint32_t *out, uint32_t B = 1,
+                           const GatherStrides &st = GatherStrides{});
 
 // --- multilinear folds (src/multilinear_poly.rs:66-87) -------------------
 // partial_eval of the top k variables (1 <= k <= 6): out (M = 2^log_len >> k
 // words) = sum_j eq(rs, j) * in[j*M + i], rs[0] for j's top bit; the k
 // challenges on the host (rs) or the device (d_rs).
+struct FoldStrides { uint64_t in = 0, out = 0, rs = 0; };
 cudaError_t fold_eq(Launcher &L, const uint32_t *in, uint32_t *out, uint32_t log_len, uint32_t k,
-                    const uint32_t *rs, const uint32_t *d_rs = nullptr);
+                    const uint32_t *rs, const uint32_t *d_rs = nullptr, uint32_t B = 1,
+                    const FoldStrides &st = FoldStrides{});
 
 struct FsTail;  // a fused transcript step, below
+// per-proof strides of the sumcheck kernels' buffers: f / g (the basis, or
+// B and bi for axpy), the folded outputs fo / go, the triple acc, the
+// challenge r (d_r / d_beta), and the fused transcript step's state (in
+// states), ticket and output words
+struct RoundStrides { uint64_t f = 0, g = 0, fo = 0, go = 0, acc = 0, r = 0, fs = 0, ticket = 0, out = 0; };
 
 // --- sumcheck rounds (src/ligerito.rs:50-127, multilinear_poly.rs:90) -----
 // acc3 (device, 3 words) is XOR-accumulated; the caller zeroes it.
 cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t log_len,
-                    uint32_t *acc3, const FsTail *tail = nullptr);
+                    uint32_t *acc3, const FsTail *tail = nullptr, uint32_t B = 1,
+                    const RoundStrides &st = RoundStrides{});
 // f, B of 2^log_len folded by r (or *d_r) into fo, Bo (2^(log_len-1));
 // triple of (fo, Bo)
 cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32_t log_len,
                        uint32_t r, uint32_t *fo, uint32_t *Bo, uint32_t *acc3, const uint32_t *d_r = nullptr,
-                       const FsTail *tail = nullptr);
+                       const FsTail *tail = nullptr, uint32_t NB = 1, const RoundStrides &st = RoundStrides{});
 // B ^= beta * bi (beta or *d_beta)
 cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta,
-                 const uint32_t *d_beta = nullptr);
+                 const uint32_t *d_beta = nullptr, uint32_t NB = 1, const RoundStrides &st = RoundStrides{});
 
 // --- induce_sumcheck_poly basis (src/sumcheck_polys.rs:74-160) ------------
 // basis[t] = sum_k apow[k] * prod_{bit i of t} S[k*n + i]; S = per-query
@@ -211,10 +229,15 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
 // The enforced sum (the sum of the setup's per-query contributions) lands
 // in d_sum (1 word).
 struct InducePlan { uint32_t b, qsplit; bool needs_zero; };
+// per-proof strides: opened rows, queries, subspace values, alpha powers
+// (2 nq words), Lo / Hi vectors, basis out, enforced sum, challenges, alpha
+struct InduceStrides {
+    uint64_t rows = 0, q = 0, S = 0, apow = 0, lo = 0, hi = 0, out = 0, sum = 0, rs = 0, alpha = 0;
+};
 InducePlan induce_plan(uint32_t n, uint32_t nq);
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
                          uint32_t n, uint32_t nq, uint32_t *d_scratch_lo, uint32_t *d_scratch_hi,
-                         uint32_t *out, uint32_t *d_sum);
+                         uint32_t *out, uint32_t *d_sum, uint32_t B = 1, const InduceStrides &st = InduceStrides{});
 
 // Per-query inputs of induce_basis from device-resident opened rows
 // (nq x glen, nq <= 2^16): S (nq x n) and, in apow (2 nq words), the alpha
@@ -224,7 +247,8 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
 cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
                          const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
                          uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs = nullptr,
-                         const uint32_t *d_alpha = nullptr);
+                         const uint32_t *d_alpha = nullptr, uint32_t B = 1,
+                         const InduceStrides &st = InduceStrides{});
 
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);
 
@@ -279,8 +303,12 @@ struct FsTail {
     uint32_t *out = nullptr;
 };
 
+// Lockstep batches: B transcripts d[0..B), one block each; per-proof
+// strides of the step / query arguments' buffers (in their elements).
+struct FsStrides { uint64_t src = 0, out = 0, mirror = 0, q = 0, nodes = 0, nnodes = 0; };
+
 // FS::new(seed)
-cudaError_t fs_init(Launcher &L, FsState *d, uint32_t seed);
+cudaError_t fs_init(Launcher &L, FsState *d, uint32_t seed, uint32_t B = 1);
 // If check: flag FS_ERR_SUMCHECK unless src[0] ^ src[1] == src[3] (a
 // sumcheck triple and its enforced sum).  Then absorb nwords u32s of src
 // (their LE bytes) and squeeze nsq field elements into out.
@@ -291,7 +319,7 @@ struct FsStep {
     uint32_t *out = nullptr;
     uint32_t *mirror = nullptr;  // when set, also receives the absorbed words
 };
-cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a);
+cudaError_t fs_step(Launcher &L, FsState *d, const FsStep &a, uint32_t B = 1, const FsStrides &st = FsStrides{});
 // Absorb nwords u32s of src; get_distinct_queries(n, s) sorted into q
 // (s <= 256, n a power of two); the multi-proof siblings of those leaves
 // in a tree of n leaves (merkle_tree::prove order) into nodes as node
@@ -310,6 +338,7 @@ struct FsQueries {
     uint32_t *out = nullptr;
     uint32_t *mirror = nullptr;  // when set, also receives the absorbed words
 };
-cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a);
+cudaError_t fs_queries(Launcher &L, FsState *d, const FsQueries &a, uint32_t B = 1,
+                       const FsStrides &st = FsStrides{});
 
 }  // namespace lgk

@@ -72,6 +72,7 @@ struct lg_server {
     std::deque<Request *> pending;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
     uint64_t next_id = 1, completed = 0;
+    uint32_t max_batch = 1;  // same-config requests a worker proves in lockstep
     bool stop = false;
     Clock::time_point t0 = Clock::now();
 
@@ -93,9 +94,17 @@ struct lg_server {
         return budget == 0 || in_flight == 0 || r->mem + in_flight + cached() <= budget;
     }
 
+    static bool same_shape(const Request *a, const Request *b) {
+        return a->len == b->len && a->on_device == b->on_device && std::memcmp(&a->cfg, &b->cfg, sizeof a->cfg) == 0;
+    }
+
     void worker(int w, lg_ctx *ctx) {
+        std::vector<Request *> batch;
+        std::vector<const uint32_t *> polys;
+        std::vector<lg_proof *> outs;
         for (;;) {
             Request *r = nullptr;
+            batch.clear();
             {
                 std::unique_lock<std::mutex> lk(mu);
                 std::deque<Request *>::iterator it;
@@ -108,20 +117,46 @@ struct lg_server {
                 r = *it;
                 pending.erase(it);
                 in_flight += r->mem;
-                r->t_start = Clock::now();
+                batch.push_back(r);
+                // queued requests of the same config join it, in queue
+                // order, while they fit the budget
+                for (auto jt = pending.begin(); jt != pending.end() && batch.size() < max_batch;) {
+                    Request *x = *jt;
+                    if ((x->worker < 0 || x->worker == w) && same_shape(x, r) && admissible(x)) {
+                        in_flight += x->mem;
+                        batch.push_back(x);
+                        jt = pending.erase(jt);
+                    } else {
+                        ++jt;
+                    }
+                }
+                const auto now = Clock::now();
+                for (auto *x : batch) x->t_start = now;
             }
-            lg_proof *p = nullptr;
-            lg_status st = lg_prove(ctx, &r->cfg, r->poly, r->len, r->on_device, &p);
+            outs.assign(batch.size(), nullptr);
+            lg_status st;
+            if (batch.size() == 1) {
+                st = lg_prove(ctx, &r->cfg, r->poly, r->len, r->on_device, &outs[0]);
+            } else {
+                polys.clear();
+                for (auto *x : batch) polys.push_back(x->poly);
+                st = lg_prove_lockstep(ctx, &r->cfg, polys.data(), r->len, (uint32_t)batch.size(), r->on_device,
+                                       outs.data());
+            }
             {
                 std::lock_guard<std::mutex> lk(mu);
-                in_flight -= r->mem;
-                r->st = st;
-                r->proof = p;
-                r->t_done = Clock::now();
-                r->done = true;
-                r->owned.clear();
-                r->owned.shrink_to_fit();
-                ++completed;
+                const auto now = Clock::now();
+                for (size_t i = 0; i < batch.size(); ++i) {
+                    Request *x = batch[i];
+                    in_flight -= x->mem;
+                    x->proof = outs[i];
+                    x->st = outs[i] ? LG_OK : (st != LG_OK ? st : LG_ERR_PROVER_ASSERT);
+                    x->t_done = now;
+                    x->done = true;
+                    x->owned.clear();
+                    x->owned.shrink_to_fit();
+                    ++completed;
+                }
             }
             cv_done.notify_all();
             cv_work.notify_all();
@@ -153,6 +188,13 @@ lg_status lg_server_create(int device, uint64_t hbm_budget_bytes, uint32_t worke
         s->threads.emplace_back([s, i, c] { s->worker((int)i, c); });
     }
     *out = s;
+    return LG_OK;
+}
+
+lg_status lg_server_set_max_batch(lg_server *s, uint32_t max_batch) {
+    if (!s || max_batch == 0 || max_batch > 64) return LG_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->max_batch = max_batch;
     return LG_OK;
 }
 

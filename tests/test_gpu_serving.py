@@ -126,3 +126,27 @@ def test_server_warm_then_same_bytes(lg, ctx):
         assert srv.wait(t)[0].to_bytes() == want
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("host_input", [False, True])
+def test_server_lockstep_batches_match_single_proofs(lg, ctx, host_input):
+    # max_batch 8: queued requests of one size are proved in lockstep
+    # groups; every proof is still the single-proof bytes
+    sizes = [16, 16, 17, 16, 18, 17, 16, 16, 17, 18, 16, 17, 16, 16, 18, 16, 17, 16, 16, 16]
+    seeds = [900 + i for i in range(len(sizes))]
+    want = _alone(lg, ctx, sizes, seeds)
+    srv = lg.Server(0, workers=2, max_batch=8)
+    try:
+        tickets = []
+        for L, s in zip(sizes, seeds):
+            cfg = lg.config_for_size(L)
+            poly = lg.splitmix_coeffs(s, cfg.poly_len) if host_input else lg.splitmix_coeffs_device(s, cfg.poly_len, ctx)
+            tickets.append(srv.submit(cfg, poly, copy_input=host_input))
+        got = [srv.wait(t)[0].to_bytes() for t in tickets]
+        assert got == want
+        st = srv.stats()
+        assert st["completed"] == len(sizes) and st["in_flight_bytes"] == 0
+    finally:
+        srv.close()
+    with pytest.raises(lg.LigeritoError):
+        lg.Server(0, workers=1, max_batch=65)
