@@ -333,8 +333,9 @@ def run_ours(args):
             # proofs batched vs looped, and a served Poisson stream vs a FIFO
             # loop at matched p99 (10,000 requests per offered rate)
             line["batch64"] = batch64(lg, 3, 1)
-            line["serve"] = serve_sweep(lg, 10000, [1000, 2000, 3000, 4000, 5000, 6000, 8000], 8,
-                                        fifo_rates=[1000, 2000, 3000, 4000])
+            line["lockstep"] = lockstep64(lg, 3, 2)
+            line["serve"] = serve_sweep(lg, 10000, [1000, 2000, 3000, 4000, 5000, 6000, 8000, 10000, 12000], 8,
+                                        fifo_rates=[1000, 2000, 3000, 4000], max_batch=8)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -496,11 +497,13 @@ def _pct(xs, q):
     return xs[min(len(xs) - 1, int(round(q * (len(xs) - 1))))] if xs else None
 
 
-def batch64(lg, steps: int, warmup: int, workers=(4, 8)) -> dict:
+def batch64(lg, steps: int, warmup: int, arms=((4, 1), (8, 1), (4, 16), (8, 8))) -> dict:
     """64 polynomials, log sizes uniform in {16..22} (seed 3), poly i from
     SplitMix64 seed 3*2^32 + i, device-resident: a loop of the plain prover
-    on one context vs the server's concurrent workers.  Wall-clock makespan
-    (host work is part of each proof), per-proof completion times."""
+    on one context vs the server's concurrent workers (arms of (workers,
+    max_batch): with max_batch > 1 a worker proves the queued requests of
+    its request's size in lockstep).  Wall-clock makespan (host work is part
+    of each proof), per-proof completion times."""
     import numpy as np
     import torch
 
@@ -532,12 +535,12 @@ def batch64(lg, steps: int, warmup: int, workers=(4, 8)) -> dict:
         loop()
     res = {"loop": [loop() for _ in range(steps)]}
     uniq = [lg.config_for_size(L) for L in sorted(set(sizes))]
-    for w in workers:
-        srv = lg.Server(0, workers=w)
+    for w, mb in arms:
+        srv = lg.Server(0, workers=w, max_batch=mb)
         srv.warm(uniq)
         for _ in range(max(1, warmup)):
             batched(srv)
-        res[f"workers{w}"] = [batched(srv) for _ in range(steps)]
+        res[f"workers{w}" + (f"_lockstep{mb}" if mb > 1 else "")] = [batched(srv) for _ in range(steps)]
         srv.close()
     ctx.close()
     out = {}
@@ -554,6 +557,44 @@ def batch64(lg, steps: int, warmup: int, workers=(4, 8)) -> dict:
             "data": "synthetic (SplitMix64), device-resident", "results": out}
 
 
+def lockstep64(lg, steps: int, warmup: int, sizes=(16, 18, 20, 22)) -> dict:
+    """64 polynomials of one size (SplitMix64 seeds 7+i), device-resident and
+    contiguous: one lg_prove_lockstep call (every kernel launch covers all
+    64 proofs) vs a loop of the plain prover on the same context.  Wall
+    clock per call, median of `steps`."""
+    import torch
+
+    ctx = lg.Context(0)
+    ctx.set_autotune(True)
+    out = {}
+    for L in sizes:
+        cfg = lg.config_for_size(L)
+        mat = torch.stack([lg.splitmix_coeffs_device(7 + i, cfg.poly_len, ctx) for i in range(64)])
+        for _ in range(max(1, warmup)):
+            lg.prove_lockstep(cfg, mat, ctx)
+            for i in range(4):
+                lg.prover(cfg, mat[i], ctx)
+        ts, tl = [], []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            lg.prove_lockstep(cfg, mat, ctx)
+            ts.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            for i in range(64):
+                lg.prover(cfg, mat[i], ctx)
+            tl.append(time.perf_counter() - t0)
+        a, b = statistics.median(ts), statistics.median(tl)
+        out[f"L{L}"] = {"lockstep_ms": round(a * 1e3, 3), "proofs_per_s": round(64 / a, 1),
+                        "loop_ms": round(b * 1e3, 3), "loop_proofs_per_s": round(64 / b, 1),
+                        "speedup": round(b / a, 2)}
+        del mat
+        torch.cuda.empty_cache()
+    ctx.close()
+    return {"workload": "lockstep64", "metric": "proofs/s of 64 same-size proofs in lockstep vs a plain GPU loop",
+            "steps": steps, "warmup": warmup, "data": "synthetic (SplitMix64), device-resident", "results": out}
+
+
 def run_batch64(args):
     sys.path.insert(0, str(ROOT))
     import __graft_entry__ as g
@@ -561,15 +602,18 @@ def run_batch64(args):
     print(json.dumps(batch64(g.load_package(), args.steps, args.warmup)), flush=True)
 
 
-def serve_sweep(lg, n_req: int, rates, workers: int, log=None, fifo_rates=None) -> dict:
+def serve_sweep(lg, n_req: int, rates, workers: int, log=None, fifo_rates=None, max_batch: int = 1) -> dict:
     """Poisson arrivals of proof requests, log sizes in {16..24} with
     P(s) ~ 2^(-(s-16)/2), coefficients SplitMix64 seed 4+i generated on the
     device as each request arrives, 160 GB admission budget.  The FIFO loop
     of the plain prover is the same server with one worker on the same
-    arrival trace.  Both arms are compared at matched p99: the FIFO arm's
-    operating point is the highest offered rate it keeps up with (at least
-    95% of the offered rate completed per second), and the served arm's is
-    the highest throughput whose p99 is no higher than that point's."""
+    arrival trace; the served arm has `workers` workers, each proving up to
+    `max_batch` queued requests of one size in lockstep.  Each arm first runs
+    1,000 unrecorded requests at its lowest rate.  Both arms are compared
+    at matched p99: the FIFO arm's operating point is the highest offered
+    rate it keeps up with (at least 95% of the offered rate completed per
+    second), and the served arm's is the highest throughput whose p99 is no
+    higher than that point's."""
     import threading
 
     import numpy as np
@@ -582,44 +626,52 @@ def serve_sweep(lg, n_req: int, rates, workers: int, log=None, fifo_rates=None) 
     cfg_by = {int(L): lg.config_for_size(int(L)) for L in svals}
     budget = 160 * 10**9
     results = []
+
+    def trace(srv, rate, n):
+        gaps = np.random.default_rng(int(rate)).exponential(1.0 / rate, size=n)
+        lat, keep, tickets = [], {}, []
+        lock = threading.Lock()
+
+        def collect():
+            for i in range(n):
+                while True:
+                    with lock:
+                        ready = i < len(tickets)
+                    if ready:
+                        break
+                    time.sleep(0.0002)
+                _, l_ms, _ = srv.wait(tickets[i])
+                lat.append(l_ms)
+                keep.pop(i, None)
+
+        th = threading.Thread(target=collect)
+        th.start()
+        t0 = time.perf_counter()
+        at = 0.0
+        for i in range(n):
+            at += gaps[i]
+            while time.perf_counter() - t0 < at:
+                pass
+            cfg = cfg_by[int(sizes[i])]
+            poly = lg.splitmix_coeffs_device(4 + i, cfg.poly_len, gen)
+            keep[i] = poly
+            t = srv.submit(cfg, poly)
+            with lock:
+                tickets.append(t)
+        th.join()
+        span = time.perf_counter() - t0
+        return {"workers": srv_workers[0], "offered_per_s": rate, "proofs_per_s": round(n / span, 1),
+                "p50_ms": round(_pct(lat, 0.5), 3), "p99_ms": round(_pct(lat, 0.99), 3)}
+
+    srv_workers = [0]
     for nw in (1, workers):
-        srv = lg.Server(0, workers=nw, hbm_budget_bytes=budget)
+        srv = lg.Server(0, workers=nw, hbm_budget_bytes=budget, max_batch=1 if nw == 1 else max_batch)
+        srv_workers[0] = nw
         srv.warm([cfg_by[int(L)] for L in svals])
-        for rate in (fifo_rates or rates) if nw == 1 else rates:
-            gaps = np.random.default_rng(int(rate)).exponential(1.0 / rate, size=n_req)
-            lat, keep, tickets = [], {}, []
-            lock = threading.Lock()
-
-            def collect():
-                for i in range(n_req):
-                    while True:
-                        with lock:
-                            ready = i < len(tickets)
-                        if ready:
-                            break
-                        time.sleep(0.0002)
-                    _, l_ms, _ = srv.wait(tickets[i])
-                    lat.append(l_ms)
-                    keep.pop(i, None)
-
-            th = threading.Thread(target=collect)
-            th.start()
-            t0 = time.perf_counter()
-            at = 0.0
-            for i in range(n_req):
-                at += gaps[i]
-                while time.perf_counter() - t0 < at:
-                    pass
-                cfg = cfg_by[int(sizes[i])]
-                poly = lg.splitmix_coeffs_device(4 + i, cfg.poly_len, gen)
-                keep[i] = poly
-                t = srv.submit(cfg, poly)
-                with lock:
-                    tickets.append(t)
-            th.join()
-            span = time.perf_counter() - t0
-            results.append({"workers": nw, "offered_per_s": rate, "proofs_per_s": round(n_req / span, 1),
-                            "p50_ms": round(_pct(lat, 0.5), 3), "p99_ms": round(_pct(lat, 0.99), 3)})
+        arm_rates = (fifo_rates or rates) if nw == 1 else rates
+        trace(srv, min(arm_rates), min(n_req, 1000))  # settles the arm; not recorded
+        for rate in arm_rates:
+            results.append(trace(srv, rate, n_req))
             if log:
                 print(json.dumps(results[-1]), file=log, flush=True)
         srv.close()
@@ -634,7 +686,8 @@ def serve_sweep(lg, n_req: int, rates, workers: int, log=None, fifo_rates=None) 
             "value": s_["proofs_per_s"] if s_ else None, "unit": "proofs/s", "higher_is_better": True,
             "speedup_vs_fifo": round(s_["proofs_per_s"] / f["proofs_per_s"], 2) if s_ else None,
             "p99_ms": s_["p99_ms"] if s_ else None, "fifo": f, "served": s_, "requests": n_req,
-            "workers": workers, "data": "synthetic (SplitMix64 seed 4+i, generated on device at arrival)",
+            "workers": workers, "max_batch": max_batch,
+            "data": "synthetic (SplitMix64 seed 4+i, generated on device at arrival)",
             "sweep": results}
 
 
@@ -643,8 +696,8 @@ def run_serve(args):
     import __graft_entry__ as g
 
     rates = [float(r) for r in args.rates.split(",")]
-    print(json.dumps(serve_sweep(g.load_package(), args.requests, rates, args.workers, log=sys.stderr)),
-          flush=True)
+    print(json.dumps(serve_sweep(g.load_package(), args.requests, rates, args.workers, log=sys.stderr,
+                                 max_batch=args.max_batch)), flush=True)
 
 
 def main():
@@ -655,18 +708,24 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="prove24",
                     choices=["prove24", "prove28", "commit24", "fft16", "fft20", "fft22", "ifft16", "ifft20", "ifft22",
-                             "batch64", "serve", "verify24"])
+                             "batch64", "lockstep64", "serve", "verify24"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=10000, help="serve: number of requests per rate")
     ap.add_argument("--rates", default="1000,2000,3000,4000,6000,8000", help="serve: offered rates (requests/s)")
     ap.add_argument("--no-mixed", action="store_true", help="prove24: skip the batch64 / serve objects")
     ap.add_argument("--no-autotune", action="store_true", help="prove24: default FFT splits and fold grid")
     ap.add_argument("--workers", type=int, default=8, help="serve: concurrent workers")
+    ap.add_argument("--max-batch", type=int, default=8, help="serve: same-size requests a worker proves in lockstep")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch64":
         run_batch64(args)
+    elif args.workload == "lockstep64":
+        sys.path.insert(0, str(ROOT))
+        import __graft_entry__ as g
+
+        print(json.dumps(lockstep64(g.load_package(), args.steps, args.warmup)), flush=True)
     elif args.workload == "serve":
         run_serve(args)
     elif args.workload == "verify24":

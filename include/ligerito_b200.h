@@ -218,7 +218,9 @@ void lg_server_destroy(lg_server *srv); /* finishes queued work first */
  * workers proving the largest size together: requests that follow pay none
  * of these first-use costs.  Waits for the proofs and discards them. */
 lg_status lg_server_warm(lg_server *srv, const lg_config *cfgs, uint32_t count);
-/* count proofs on `workers` concurrent contexts; out[i] as lg_prove */
+/* count proofs on `workers` concurrent contexts, same-config proofs in
+ * lockstep groups of up to 8 (lg_server_set_max_batch); out[i] as
+ * lg_prove */
 lg_status lg_prove_batch(int device, uint32_t workers, const lg_config *cfgs, const uint32_t *const *polys,
                          const uint64_t *lens, int polys_on_device, uint32_t count, lg_proof **out);
 

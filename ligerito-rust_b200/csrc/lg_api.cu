@@ -324,17 +324,36 @@ Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
     return w;
 }
 
+// Copy groups of the host-input commitment (column counts, in order): the
+// columns form hash units of 16 (one BLAKE3 block of every leaf); the
+// first unit arrives as 1/4, 1/4, 1/2 of it so that compute starts after
+// a few columns, the last as two halves so that little work remains after
+// the last bytes land, the units between whole.
+std::vector<uint32_t> host_copy_groups(uint32_t n) {
+    const uint32_t U = std::min<uint32_t>(16, n), units = (n + U - 1) / U;
+    std::vector<uint32_t> g;
+    for (uint32_t u = 0; u < units; ++u) {
+        const uint32_t cols = std::min(U, n - u * U);
+        if (u == 0 && cols >= 8 && cols % 4 == 0) {
+            g.insert(g.end(), {cols / 4, cols / 4, cols / 2});
+        } else if (u + 1 == units && cols >= 8 && cols % 2 == 0) {
+            g.insert(g.end(), {cols / 2, cols / 2});
+        } else {
+            g.push_back(cols);
+        }
+    }
+    return g;
+}
+
 // The first commitment of a proof whose polynomial is on the host: the
-// columns travel in groups of 16 on the copy stream; the compute stream
-// waits for each group and, while the next group is in flight, runs its
-// scale-and-spread and the FFT passes but the last (columns are
-// independent).  Each pair of groups then gets the last FFT pass and its
-// BLAKE3 blocks of every leaf: a leaf is the row's words in column order
-// and 16 words are one BLAKE3 block, so group g is block g of each leaf's
-// chunk, chained through the leaf slots of the tree.  Pairs, because the
-// last pass builds its node tables per tile of vectors and 32 columns
-// share them better than 16.  After the last pair only the upper tree
-// remains.
+// columns travel in groups (host_copy_groups) on the copy stream; the
+// compute stream waits for each group and, while the next is in flight,
+// runs its scale-and-spread and the FFT passes but the last (columns are
+// independent).  Each hash unit of 16 columns, once all its groups are
+// in, gets the last FFT pass and its BLAKE3 block of every leaf: a leaf is
+// the row's words in column order and 16 words are one BLAKE3 block, so
+// unit u is block u of each leaf's chunk, chained through the leaf slots
+// of the tree.  After the last unit only the upper tree remains.
 Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_t *d_poly, uint32_t log_m,
                          uint32_t n) {
     const Code code = get_code(c, log_m);
@@ -347,7 +366,8 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
     cudaPointerAttributes attr{};
     const bool pinned_src = cudaPointerGetAttributes(&attr, h_poly) == cudaSuccess && attr.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    const uint32_t group = std::min<uint32_t>(n, 16), ngroups = (n + group - 1) / group;
+    const std::vector<uint32_t> groups = host_copy_groups(n);
+    const uint32_t U = std::min<uint32_t>(16, n);
     DBuf scaled(c, log_m > 6 ? 4ull * n * m : 0);
     // staging for pageable input: two pinned chunks, reused after their copy
     constexpr size_t kChunk = 4u << 20;
@@ -359,8 +379,9 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
     // compute stream that may still read d_poly's memory
     CK(c, cudaEventRecord(c->copy_ev[7], c->stream));
     CK(c, cudaStreamWaitEvent(c->copy_stream, c->copy_ev[7], 0));
-    for (uint32_t g = 0; g < ngroups; ++g) {
-        const uint32_t j0 = g * group, cols = std::min(group, n - j0);
+    uint32_t j0 = 0;
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const uint32_t cols = groups[g];
         const uint8_t *src = reinterpret_cast<const uint8_t *>(h_poly + (uint64_t)j0 * m);
         uint8_t *dst = reinterpret_cast<uint8_t *>(d_poly + (uint64_t)j0 * m);
         const size_t bytes = (size_t)cols * m * 4;
@@ -383,11 +404,12 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
         uint32_t *Eg = w.E.u32() + (uint64_t)j0 * rows;
         rs_encode(c, code, d_poly + (uint64_t)j0 * m, log_m, cols, Eg, rows, scaled.u32() + (uint64_t)j0 * m,
                   lgk::FFT_HEAD);
-        if (g % 2 == 1 || g + 1 == ngroups) {
-            const uint32_t gp = g - g % 2, jp = gp * group, pcols = j0 + cols - jp;
-            CK(c, lgk::fft_vectors(c->L, w.E.u32() + (uint64_t)jp * rows, code.tw, log_m, pcols, rows, 4, m, 4, false,
+        j0 += cols;
+        if (j0 % U == 0 || j0 == n) {  // a hash unit is complete
+            const uint32_t u = (j0 - 1) / U, ju = u * U, ucols = j0 - ju;
+            CK(c, lgk::fft_vectors(c->L, w.E.u32() + (uint64_t)ju * rows, code.tw, log_m, ucols, rows, 4, m, 4, false,
                                    lgk::FFT_LAST));
-            CK(c, lgk::leaf_hash_block(c->L, w.E.u32(), rows, n, gp, g - gp + 1, w.tree.u32()));
+            CK(c, lgk::leaf_hash_block(c->L, w.E.u32(), rows, n, u, 1, w.tree.u32()));
         }
     }
     CK(c, lgk::merkle_upper(c->L, w.tree.u32(), rows));
@@ -1715,6 +1737,16 @@ lg_status lg_prove_lockstep(lg_ctx *c, const lg_config *cfg, const uint32_t *con
         st = guarded(c, [&] {
             CK(c, cudaSetDevice(c->device));
             Scratch sc(c);
+            if (B == 1) {  // alone, the single-proof path is faster
+                bad.assign(1, 0);
+                if (on_device) prove_impl(c, sc, *cfg, polys[s0], len, res[0]->p);
+                else {
+                    DBuf one(c, len * 4);
+                    prove_impl(c, sc, *cfg, one.u32(), len, res[0]->p, polys[s0]);
+                }
+                sc.finish();
+                return;
+            }
             // the inputs as one contiguous run, copied together unless
             // they already are
             bool contiguous = on_device != 0;

@@ -56,9 +56,12 @@ __global__ void k_fs_step(FsState *g, FsStep a, FsStrides st) {
     __shared__ FsState S;
     __shared__ Batch B;
     __shared__ uint32_t stage[32];
+    __shared__ uint32_t kw[kKwBlocks][64];
     load_state(S, g);
     const bool bad = threadIdx.x == 0 && a.check && (a.src[0] ^ a.src[1]) != a.src[3];
-    fs_absorb_block(S, a.src, a.nwords, stage, 32, a.mirror);
+    // long runs (yr) with the message schedules in parallel
+    if (a.nwords >= 64) fs_absorb_sched(S, a.src, a.nwords, kw, a.mirror);
+    else fs_absorb_block(S, a.src, a.nwords, stage, 32, a.mirror);
     if (bad) S.err |= FS_ERR_SUMCHECK;
     __syncthreads();
     fs_fields(S, B, a.nsq, a.out);

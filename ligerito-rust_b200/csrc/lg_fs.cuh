@@ -130,6 +130,48 @@ __device__ void fs_absorb_block(FsState &S, const uint32_t *src, uint32_t nwords
     }
 }
 
+// The whole block absorbs a long run of nwords u32s from device memory:
+// the words up to the first SHA-256 block boundary and after the last one
+// go through fs_absorb on thread 0, and the whole blocks between have
+// their message schedules computed in parallel (one block per thread,
+// kKwBlocks at a time, into kw) so that thread 0 runs only the 64 rounds
+// of each.  A non-null mirror receives a copy of the words.
+constexpr uint32_t kKwBlocks = 32;
+__device__ void fs_absorb_sched(FsState &S, const uint32_t *src, uint32_t nwords, uint32_t (*kw)[64],
+                                uint32_t *mirror) {
+    const uint32_t head = min(nwords, (16u - S.nw) & 15u);
+    const uint32_t full = (nwords - head) / 16, done = head + 16 * full;
+    if (threadIdx.x == 0) fs_absorb(S, src, head);
+    if (mirror)
+        for (uint32_t i = threadIdx.x; i < head; i += blockDim.x) mirror[i] = src[i];
+    __syncthreads();
+    for (uint32_t b0 = 0; b0 < full; b0 += kKwBlocks) {
+        const uint32_t nb = min(kKwBlocks, full - b0);
+        for (uint32_t t = threadIdx.x; t < nb; t += blockDim.x) {
+            const uint32_t off = head + 16 * (b0 + t);
+            uint32_t blk[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const uint32_t v = src[off + k];
+                if (mirror) mirror[off + k] = v;
+                blk[k] = bswap32(v);
+            }
+            sha_schedule_kw(blk, kw[t]);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (uint32_t i = 0; i < nb; ++i) sha_rounds_kw(S.h, kw[i]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        S.total += 64ull * full;
+        fs_absorb(S, src + done, nwords - done);
+    }
+    if (mirror)
+        for (uint32_t i = done + threadIdx.x; i < nwords; i += blockDim.x) mirror[i] = src[i];
+    __syncthreads();
+}
+
 // Word j of the pending words followed by the counters c, c+1, ... (each
 // counter's LE bytes as a big-endian message word).
 __device__ __forceinline__ uint32_t stream_word(const FsState &S, uint32_t j) {

@@ -334,6 +334,9 @@ lg_status lg_server_warm(lg_server *s, const lg_config *cfgs, uint32_t count) {
     return st;
 }
 
+// same-config proofs lg_prove_batch runs in lockstep on one worker
+constexpr uint32_t kBatchLockstep = 8;
+
 lg_status lg_prove_batch(int device, uint32_t workers, const lg_config *cfgs, const uint32_t *const *polys,
                          const uint64_t *lens, int polys_on_device, uint32_t count, lg_proof **out) {
     if (!cfgs || !polys || !lens || !out) return LG_ERR_INVALID_ARGUMENT;
@@ -341,6 +344,7 @@ lg_status lg_prove_batch(int device, uint32_t workers, const lg_config *cfgs, co
     lg_server *s = nullptr;
     lg_status st = lg_server_create(device, 0, std::max<uint32_t>(1, std::min(workers, count)), &s);
     if (st != LG_OK) return st;
+    lg_server_set_max_batch(s, kBatchLockstep);
     std::vector<uint64_t> tickets(count);
     lg_status first = LG_OK;
     for (uint32_t i = 0; i < count; ++i) {
