@@ -1032,6 +1032,20 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
     __shared__ __align__(512) uint32_t tabs[NH + NL][kTabWords];  // EL tables, then EH
     __shared__ uint32_t r[KH + KL];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // V consecutive outputs per thread (16-byte loads for V = 4)
+    const uint64_t groups = M / V, gstride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    // V = 1: all 2^k inputs of an output are loaded at once, the first
+    // output's before the tables are built and the next one's right after
+    // the current one's products, so that the loads' HBM latency overlaps
+    // the table builds and the products
+    constexpr int NV = V == 1 ? NH * NL : 1;
+    uint32_t pre[NV];
+    auto load_all = [&](uint64_t gg) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) pre[j] = __ldg(in + gg + (uint64_t)j * M);
+    };
+    if (V == 1 && g < groups) load_all(g);
     if (threadIdx.x < KH + KL) r[threadIdx.x] = d_rs ? d_rs[threadIdx.x] : rs.v[threadIdx.x];
     __syncthreads();
     // evaluate_lagrange_basis (src/utils.rs:4-27) of each half: entry j has
@@ -1046,10 +1060,22 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
     }
     __syncthreads();
     const uint8_t *t8 = reinterpret_cast<const uint8_t *>(&tabs[0][0]);
-    // V consecutive outputs per thread (16-byte loads for V = 4)
-    const uint64_t groups = M / V;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
-         g += (uint64_t)gridDim.x * blockDim.x) {
+    if constexpr (V == 1) {
+        for (; g < groups; g += gstride) {
+            uint32_t acc = 0;
+#pragma unroll
+            for (int jh = 0; jh < NH; ++jh) {
+                uint32_t part = 0;
+#pragma unroll
+                for (int jl = 0; jl < NL; ++jl) part ^= tab_mul_sa(t8, 512u * jl, 0, pre[jh * NL + jl]);
+                acc ^= KH ? tab_mul_sa(t8, 512u * (NL + jh), 0, part) : part;
+            }
+            if (g + gstride < groups) load_all(g + gstride);
+            out[g] = acc;
+        }
+        return;
+    }
+    for (; g < groups; g += gstride) {
         const uint32_t *src = in + g * V;
         uint32_t acc[V];
 #pragma unroll
@@ -1060,13 +1086,8 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
 #pragma unroll
             for (int jl = 0; jl < NL; ++jl) {
                 const uint32_t *p = src + (uint64_t)(jh * NL + jl) * M;
-                if constexpr (V == 4) {
-                    const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
-                    v[jl][0] = t.x; v[jl][1] = t.y; v[jl][2] = t.z; v[jl][3] = t.w;
-                } else {
-#pragma unroll
-                    for (int x = 0; x < V; ++x) v[jl][x] = __ldg(p + x);
-                }
+                const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+                v[jl][0] = t.x; v[jl][1] = t.y; v[jl][2] = t.z; v[jl][3] = t.w;
             }
 #pragma unroll
             for (int x = 0; x < V; ++x) {
@@ -1076,12 +1097,7 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
                 acc[x] ^= KH ? tab_mul_sa(t8, 512u * (NL + jh), 0, part) : part;
             }
         }
-        if constexpr (V == 4) {
-            *reinterpret_cast<uint4 *>(out + g * 4) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
-        } else {
-#pragma unroll
-            for (int x = 0; x < V; ++x) out[g * V + x] = acc[x];
-        }
+        *reinterpret_cast<uint4 *>(out + g * 4) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
     }
 }
 
