@@ -1288,11 +1288,9 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
 InducePlan induce_plan(uint32_t n, uint32_t nq) {
     InducePlan p;
     p.b = std::min<uint32_t>(n, 9);
-    const uint64_t blocks_t = 1ull << (n - p.b);
-    uint32_t qs = 1;
-    while (blocks_t * qs < 3 * 296 && qs * 16 < nq) qs *= 2;  // about 3 waves of 2 blocks per SM
-    p.qsplit = qs;
-    p.needs_zero = qs > 1;
+    p.qsplit = 1;          // work is split evenly over one wave of blocks instead
+    p.needs_zero = false;  // induce_prep zeroes the output
+    (void)nq;
     return p;
 }
 
@@ -1379,7 +1377,7 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
 // larger ones double in place in global memory.
 __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__restrict__ apow, uint32_t n,
                               uint32_t b, uint32_t nq, uint32_t *__restrict__ lo, uint32_t *__restrict__ hi,
-                              uint32_t *sum_out, int in_smem, InduceStrides st) {
+                              uint32_t *sum_out, int in_smem, uint32_t *__restrict__ out, InduceStrides st) {
     pdl_begin();
     {
         const uint32_t pb = blockIdx.y;  // lockstep batch: proof pb
@@ -1388,7 +1386,12 @@ __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__
         lo += pb * st.lo;
         hi += pb * st.hi;
         sum_out += pb * st.sum;
+        out += pb * st.out;
     }
+    // induce_main XORs its partial sums into the basis: zero it first
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (1ull << n);
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = 0;
     extern __shared__ uint32_t sbuf[];  // Lo then Hi, when in_smem
     __shared__ uint32_t Ss[32];          // the query's subspace values, read once
     const uint32_t k = blockIdx.x, nlo = 1u << b, nhi = 1u << (n - b);
@@ -1423,63 +1426,99 @@ __global__ void k_induce_prep(const uint32_t *__restrict__ S, const uint32_t *__
     }
 }
 
+// basis[(t_hi << b) | t_lo] = sum_k Hi_k[t_hi] * Lo_k[t_lo].  Work items are
+// the (proof, t_hi, query) triples in that order; block i takes the
+// contiguous range [i P / G, (i+1) P / G) of the P triples, so one wave of
+// blocks gets equal shares (no partial last wave).  A range splits into
+// segments of one (proof, t_hi): each warp takes every 8th query of the
+// segment, builds the table of Hi_k[t_hi] and multiplies it into its
+// lane's share of Lo_k; at the segment's end the warps' sums meet in
+// shared memory and go to out (zeroed by induce_prep) by store when the
+// segment covers all queries, else by XOR.
 template <int ACC>  // ACC = max(1, 2^b / 32) words per lane
-__global__ void __launch_bounds__(256) k_induce_main(const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
-                                                     uint32_t n, uint32_t b, uint32_t nq, uint32_t qs,
-                                                     uint32_t *__restrict__ out, int atomic_out, InduceStrides st) {
+__global__ void __launch_bounds__(256, ACC <= 16 ? 3 : 2) k_induce_main(const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
+                                                     uint32_t n, uint32_t b, uint32_t nq, uint32_t B,
+                                                     uint32_t *__restrict__ out, InduceStrides st) {
     pdl_begin();
-    lo += blockIdx.z * st.lo;  // lockstep batch: proof blockIdx.z
-    hi += blockIdx.z * st.hi;
-    out += blockIdx.z * st.out;
     __shared__ __align__(128) uint32_t tabs[8][kTabWords];
     __shared__ uint32_t red[32 * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const uint32_t tb = blockIdx.x, nlo = 1u << b, nhi = 1u << (n - b);
-    const uint32_t per = (nq + qs - 1) / qs, k0 = blockIdx.y * per, k1 = min(nq, k0 + per);
-    uint32_t acc[ACC], cur[ACC], nxt[ACC];
+    const uint32_t nlo = 1u << b, nhi = 1u << (n - b);
+    const uint64_t P = (uint64_t)B * nhi * nq;
+    uint64_t p = blockIdx.x * P / gridDim.x;
+    const uint64_t pend = (blockIdx.x + 1) * P / gridDim.x;
+    while (p < pend) {
+        const uint64_t seg = p / nq;
+        const uint32_t k0 = (uint32_t)(p - seg * nq);
+        const uint64_t left = pend - p;
+        const uint32_t k1 = left < (uint64_t)(nq - k0) ? k0 + (uint32_t)left : nq;
+        const uint32_t pb = (uint32_t)(seg / nhi), tb = (uint32_t)(seg - (uint64_t)pb * nhi);
+        const uint32_t *lop = lo + pb * st.lo, *hip = hi + pb * st.hi;
+        uint32_t acc[ACC], va[ACC], vb[ACC];
 #pragma unroll
-    for (int c = 0; c < ACC; ++c) acc[c] = cur[c] = nxt[c] = 0;
-    // the next query's Hi value and Lo vector are loaded while the current
-    // one is multiplied (the loads come from L2 and would otherwise stall)
-    auto load = [&](uint32_t k, uint32_t (&v)[ACC]) {
-        const uint32_t *lk = lo + (uint64_t)k * nlo;
+        for (int c = 0; c < ACC; ++c) acc[c] = va[c] = vb[c] = 0;
+        // (ACC > 1 means nlo = 32 ACC: every lane word is in range)
+        auto in_range = [&](int c) { return ACC > 1 || lane + 32u * c < nlo; };
+        // the next query's Hi value and Lo vector are loaded while the
+        // current one is multiplied (the loads come from L2); the two
+        // register sets swap roles by unrolling the query loop twice
+        auto load = [&](uint32_t k, uint32_t (&v)[ACC]) {
+            const uint32_t *lk = lop + (uint64_t)k * nlo + lane;
 #pragma unroll
-        for (int c = 0; c < ACC; ++c) {
-            const uint32_t u = lane + 32 * c;
-            if (u < nlo) v[c] = __ldg(lk + u);
+            for (int c = 0; c < ACC; ++c)
+                if (in_range(c)) v[c] = __ldg(lk + 32 * c);
+            return __ldg(hip + (uint64_t)k * nhi + tb);
+        };
+        auto step = [&](uint32_t k, uint32_t h, const uint32_t (&v)[ACC], uint32_t (&nv)[ACC], uint32_t &hn) {
+            if (k + nw < k1) hn = load(k + nw, nv);
+            tab_build_warp(tabs[warp], h, lane);
+            __syncwarp();
+#pragma unroll
+            for (int c = 0; c < ACC; ++c)
+                if (in_range(c)) acc[c] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * warp, 0, v[c]);
+            __syncwarp();
+        };
+        uint32_t k = k0 + warp, ha = 0, hb = 0;
+        if (k < k1) ha = load(k, va);
+        for (; k < k1; k += 2 * nw) {
+            step(k, ha, va, vb, hb);
+            if (k + nw >= k1) break;
+            step(k + nw, hb, vb, va, ha);
         }
-        return __ldg(hi + (uint64_t)k * nhi + tb);
-    };
-    uint32_t k = k0 + warp, hcur = 0;
-    if (k < k1) hcur = load(k, cur);
-    for (; k < k1; k += nw) {
-        uint32_t hnxt = 0;
-        if (k + nw < k1) hnxt = load(k + nw, nxt);
-        tab_build_warp(tabs[warp], hcur, lane);
-        __syncwarp();
+        for (uint32_t w = threadIdx.x; w < nlo; w += blockDim.x) red[w] = 0;
+        __syncthreads();
 #pragma unroll
-        for (int c = 0; c < ACC; ++c) {
-            const uint32_t u = lane + 32 * c;
-            if (u < nlo) acc[c] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(tabs), 512u * warp, 0, cur[c]);
+        for (int c = 0; c < ACC; ++c)
+            if (in_range(c)) atomicXor(&red[lane + 32 * c], acc[c]);
+        __syncthreads();
+        uint32_t *dst = out + pb * st.out + (uint64_t)tb * nlo;
+        const bool whole = k0 == 0 && k1 == nq;
+        for (uint32_t w = threadIdx.x; w < nlo; w += blockDim.x) {
+            if (whole) dst[w] = red[w];
+            else atomicXor(dst + w, red[w]);
         }
-        __syncwarp();
-        hcur = hnxt;
-#pragma unroll
-        for (int c = 0; c < ACC; ++c) cur[c] = nxt[c];
+        __syncthreads();  // red is reused by the next segment
+        p += k1 - k0;
     }
-    for (uint32_t w = threadIdx.x; w < nlo; w += blockDim.x) red[w] = 0;
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < ACC; ++c) {
-        const uint32_t u = lane + 32 * c;
-        if (u < nlo) atomicXor(&red[u], acc[c]);
+}
+
+// One wave of induce_main blocks (occupancy of the instantiation, cached).
+template <int ACC>
+static unsigned induce_grid(uint64_t work) {
+    static std::atomic<int> occ_c{0}, sms_c{0};
+    int sms = sms_c.load(std::memory_order_relaxed), o = occ_c.load(std::memory_order_relaxed);
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+        sms_c.store(sms, std::memory_order_relaxed);
     }
-    __syncthreads();
-    uint32_t *dst = out + (uint64_t)tb * nlo;
-    for (uint32_t w = threadIdx.x; w < nlo; w += blockDim.x) {
-        if (atomic_out) atomicXor(dst + w, red[w]);
-        else dst[w] = red[w];
+    if (!o) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_induce_main<ACC>, 256, 0) != cudaSuccess || o < 1) o = 1;
+        occ_c.store(o, std::memory_order_relaxed);
     }
+    // at least 32 (proof, t_hi, query) triples a block, so its 8 warps all work
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((work + 31) / 32, (uint64_t)sms * o));
 }
 
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
@@ -1491,15 +1530,14 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
     const size_t words = (1ull << p.b) + (1ull << (n - p.b));
     const int in_smem = words <= 12288;  // 48 KB: no opt-in needed
     LGK_LAUNCH(L, "induce_prep", launch_k(k_induce_prep, dim3(nq, B), 256, in_smem ? 4 * words : 0, L.stream, d_S,
-                                          d_apow, n, p.b, nq, d_lo, d_hi, d_sum, in_smem, st));
+                                          d_apow, n, p.b, nq, d_lo, d_hi, d_sum, in_smem, out, st));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 grid(1u << (n - p.b), p.qsplit, B);
-    const int ao = p.qsplit > 1;
+    const uint64_t work = (uint64_t)B * (1ull << (n - p.b)) * nq;
     L.note(4.0 * B * (vec + (1ull << n)), (double)B * nq * (1ull << n));
     switch (std::max<uint32_t>(1, (1u << p.b) / 32)) {
 #define LGK_CASE(a) \
-    case a: LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main<a>, grid, 256, 0, L.stream, d_lo, d_hi, n, p.b, nq, p.qsplit, out, ao, st)); break;
+    case a: LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main<a>, induce_grid<a>(work), 256, 0, L.stream, d_lo, d_hi, n, p.b, nq, B, out, st)); break;
         LGK_CASE(1) LGK_CASE(2) LGK_CASE(4) LGK_CASE(8) LGK_CASE(16) LGK_CASE(32)
 #undef LGK_CASE
         default: return cudaErrorInvalidValue;

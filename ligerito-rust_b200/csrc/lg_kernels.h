@@ -224,8 +224,8 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
 
 // --- induce_sumcheck_poly basis (src/sumcheck_polys.rs:74-160) ------------
 // basis[t] = sum_k apow[k] * prod_{bit i of t} S[k*n + i]; S = per-query
-// subspace values (sks_at_x).  out (2^n) must be zeroed when it returns
-// needs_zero = true.
+// subspace values (sks_at_x).  induce_basis writes all of out (2^n words);
+// a plan with needs_zero set (none currently) wants out zeroed first.
 // The enforced sum (the sum of the setup's per-query contributions) lands
 // in d_sum (1 word).
 struct InducePlan { uint32_t b, qsplit; bool needs_zero; };
