@@ -58,7 +58,7 @@ struct lg_ctx {
     size_t pinned_cap = 0;
     // per-call bump arenas (reset at the start of each prove / verify)
     uint8_t *pin_arena = nullptr;
-    size_t pin_cap = 0, pin_used = 0;
+    size_t pin_cap = 0, pin_used = 0, pin_want = 0;  // pin_want: the arena a call wanted
     uint8_t *dev_arena = nullptr;
     size_t dev_cap = 0, dev_used = 0;
 };
@@ -183,7 +183,9 @@ const uint32_t *get_fft_tw(lg_ctx *c, uint32_t log_n) {
 
 // ------------------------------------------------------------- scratch
 // Per-call scratch: small device buffers come from a bump arena, uploads
-// and downloads go through a pinned bump arena without synchronising, and
+// and downloads go through a pinned bump arena without synchronising (a
+// call that outgrows it gets extra pinned blocks, valid until the call
+// ends, and the next call starts with an arena that size), and
 // host-side results of downloads (openings) are materialised by finalizers
 // after the call's last synchronisation.  Deferred downloads (of arena
 // buffers, which live until the call ends) are only queued by flush(), so
@@ -192,15 +194,21 @@ const uint32_t *get_fft_tw(lg_ctx *c, uint32_t log_n) {
 struct Scratch {
     lg_ctx *c;
     std::vector<DBuf> dev_overflow;
+    std::vector<uint8_t *> pin_overflow;
     std::vector<std::function<void()>> finalizers;
     struct Deferred { uint8_t *h; const void *d; size_t bytes; };
     std::vector<Deferred> deferred;
     static constexpr size_t kPin = 8u << 20, kDevArena = 32u << 20;
     explicit Scratch(lg_ctx *ctx) : c(ctx) {
         constexpr size_t kDev = kDevArena;
+        if (c->pin_arena && c->pin_want > c->pin_cap) {  // the last call outgrew it; nothing is in flight
+            cudaFreeHost(c->pin_arena);
+            c->pin_arena = nullptr;
+        }
         if (!c->pin_arena) {
-            CK(c, cudaMallocHost((void **)&c->pin_arena, kPin));
-            c->pin_cap = kPin;
+            const size_t cap = std::max(kPin, (c->pin_want + (1u << 20) - 1) & ~size_t((1u << 20) - 1));
+            CK(c, cudaMallocHost((void **)&c->pin_arena, cap));
+            c->pin_cap = cap;
         }
         if (!c->dev_arena) {
             CK(c, cudaMalloc((void **)&c->dev_arena, kDev));
@@ -219,23 +227,29 @@ struct Scratch {
         sync(c);
         for (auto &f : finalizers) f();
         finalizers.clear();
-        c->pin_used = 0;
     }
+    // Pinned host bytes valid until the call ends (earlier ones stay valid:
+    // the arena is never reused or moved within a call).
     uint8_t *pin(size_t bytes) {
         bytes = (bytes + 63) & ~size_t(63);
+        c->pin_want = std::max(c->pin_want, c->pin_used + bytes);
         if (c->pin_used + bytes > c->pin_cap) {
-            finish();  // drains every transfer that uses the arena
-            if (bytes > c->pin_cap) {
-                cudaFreeHost(c->pin_arena);
-                c->pin_arena = nullptr;
-                size_t cap = std::max(bytes, 2 * c->pin_cap);
-                CK(c, cudaMallocHost((void **)&c->pin_arena, cap));
-                c->pin_cap = cap;
-            }
+            uint8_t *p = nullptr;
+            CK(c, cudaMallocHost((void **)&p, bytes));
+            pin_overflow.push_back(p);
+            c->pin_used += bytes;  // counted, so the next call's arena covers it
+            return p;
         }
         uint8_t *p = c->pin_arena + c->pin_used;
         c->pin_used += bytes;
         return p;
+    }
+    ~Scratch() {
+        if (pin_overflow.empty()) return;
+        // copies into the extra blocks may still be in flight after an error
+        cudaStreamSynchronize(c->stream);
+        if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+        for (uint8_t *p : pin_overflow) cudaFreeHost(p);
     }
     void *dev(size_t bytes) {
         bytes = (bytes + 255) & ~size_t(255);

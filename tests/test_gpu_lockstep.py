@@ -86,3 +86,17 @@ def test_lockstep_reports_like_single_prover(lg, ctx):
     # the context still proves afterwards
     m2, r2 = _stack(lg, ctx, good, [11, 12])
     assert [p.to_bytes() for p in lg.prove_lockstep(good, m2, ctx)] == _single(lg, ctx, good, r2)
+
+
+def test_lockstep_64_large_group(lg, ctx):
+    # 64 proofs at 2^20: the openings outgrow the context's pinned arena
+    # (about 9 MiB for the first opening alone), so the call spills to
+    # extra pinned blocks; members still equal their single proofs
+    cfg = lg.config_for_size(20)
+    mat, rows = _stack(lg, ctx, cfg, [5000 + i for i in range(64)])
+    got = lg.prove_lockstep(cfg, mat, ctx)
+    pick = (0, 17, 63)
+    assert [got[i].to_bytes() for i in pick] == _single(lg, ctx, cfg, [rows[i] for i in pick])
+    # and again: the next call starts with an arena of the size this one used
+    got2 = lg.prove_lockstep(cfg, mat, ctx)
+    assert [got2[i].to_bytes() for i in pick] == [got[i].to_bytes() for i in pick]
