@@ -159,11 +159,15 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a,
     // get_distinct_queries in batches of squeezes; the round bound only
     // guards a state that cannot progress (n >= s always can)
     for (uint32_t round = 0; ok && count < a.s && round < 1024; ++round) {
-        // a few more squeezes than queries still needed plus the challenges
-        // squeezed after them: the chain of full blocks a batch completes
-        // is its serial part
+        // the queries still needed, about twice the repeats expected among
+        // them (need (need/2 + count) / n) plus 2 more, and the challenges
+        // squeezed after them: the chain of full blocks a batch completes is
+        // its serial part (~1.2 us a block), so the batch is kept tight; a
+        // short batch just takes another round
         const uint32_t need = a.s - count;
-        batch = min(kQBlock, need + need / 16 + 8 + a.nsq);
+        const uint64_t margin = ((uint64_t)need * (need + 2ull * count)) / a.n + 2;
+        const uint64_t want = need + margin + a.nsq;
+        batch = want < kQBlock ? (uint32_t)want : kQBlock;
         fs_chain_block(S, B, batch, kw);
         uint64_t qv = 0;
         if (tid < batch) {

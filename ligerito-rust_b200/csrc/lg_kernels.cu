@@ -1288,7 +1288,6 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
 InducePlan induce_plan(uint32_t n, uint32_t nq) {
     InducePlan p;
     p.b = std::min<uint32_t>(n, 9);
-    p.qsplit = 1;          // work is split evenly over one wave of blocks instead
     p.needs_zero = false;  // induce_prep zeroes the output
     (void)nq;
     return p;

@@ -228,7 +228,7 @@ cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len,
 // a plan with needs_zero set (none currently) wants out zeroed first.
 // The enforced sum (the sum of the setup's per-query contributions) lands
 // in d_sum (1 word).
-struct InducePlan { uint32_t b, qsplit; bool needs_zero; };
+struct InducePlan { uint32_t b; bool needs_zero; };  // b: low bits of t in Lo
 // per-proof strides: opened rows, queries, subspace values, alpha powers
 // (2 nq words), Lo / Hi vectors, basis out, enforced sum, challenges, alpha
 struct InduceStrides {

@@ -227,3 +227,23 @@ def test_launch_count_and_timing(lg, ctx):
     assert {"leaf_hash", "fold_round", "induce_main", "fs_queries"} <= set(stats)
     assert any(k.startswith("merkle_") for k in stats)
     assert any(k.startswith("fft_pass_L") for k in stats)
+
+
+# Witnesses of 512 and 1024 rows opened by the device transcript: 148
+# distinct queries among 512 rows take the most squeezes and sometimes a
+# second batch (the batch is sized by the repeats expected).
+SMALL_ROWS = {
+    "initial512": (1, 7, 2, [6], [1]),
+    "step512": (2, 9, 2, [7, 6], [2, 1]),
+    "steps1024_512": (3, 9, 1, [8, 7, 6], [1, 1, 1]),
+}
+
+
+@pytest.mark.parametrize("name", list(SMALL_ROWS))
+def test_small_row_openings_match_oracle(lg, ref, ctx, name):
+    steps, lm0, ln0, lm, ln = SMALL_ROWS[name]
+    pc = lg.ProverConfig(steps, (1 << lm0, 1 << ln0), [(1 << m, 1 << n) for m, n in zip(lm, ln)], ln0, list(ln))
+    rc = ref.config(steps, lm0, ln0, lm, ln)
+    for seed in range(6):
+        poly = lg.splitmix_coeffs(700 + seed, pc.poly_len)
+        assert lg.prover(pc, lg.to_device(poly), ctx).to_bytes() == ref.prove(rc, poly, nthreads=4), seed
