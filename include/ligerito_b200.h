@@ -150,6 +150,38 @@ lg_status lg_measure_pipe_peaks(int device, double *rates, uint32_t count);
 lg_status lg_prove(lg_ctx *ctx, const lg_config *cfg, const uint32_t *poly, uint64_t len,
                    int poly_on_device, lg_proof **out);
 
+/* Debug / parity: the same proof as lg_prove, handing each intermediate of
+ * src/prover.rs:15-199 to `cb` as soon as the device has produced it (the
+ * call synchronises at every one, so it is much slower than lg_prove).
+ * `data` is a host copy valid only during the callback.  Names and levels
+ * (level = recursion depth of the commitment or opening; round = global
+ * sumcheck round; triple = index in the proof's transcript order):
+ *   "twiddles" / "pis"      level  ReedSolomonEncoding::new tables, u32
+ *                                  (reed_solomon.rs:49-64)
+ *   "encoded" / "tree"      level  ligero_commit: column-major encoded
+ *                                  matrix (u32) and all Merkle layers,
+ *                                  leaves first, 32 B per node (ligero.rs:70-95)
+ *   "fold_challenges"       0      the initial_k partial_eval challenges
+ *   "folded"                0      partial_eval(poly, challenges) (prover.rs:52-53)
+ *   "queries"               level  sorted distinct queries opened on that
+ *                                  commitment, u64 (emulated_fs.rs:62-75)
+ *   "opened_rows"           level  their rows, row-major u32 (ligero.rs:40-51)
+ *   "alpha"                 level  the induce challenge (prover.rs:68,158)
+ *   "basis" / "enforced_sum" level induce_sumcheck_poly_parallel's output
+ *                                  (sumcheck_polys.rs:83-160)
+ *   "triple"                triple (s0, s1, s2) of eval_013 / eval_01x
+ *   "round_challenge"       round  the fold challenge of that round
+ *   "round_f" / "round_basis" round f and the summed basis after the fold
+ *                                  (ligerito.rs:119-127; the reference folds
+ *                                  each basis polynomial, whose sum this is)
+ *   "beta" / "basis_sum"    level  the glue challenge and the summed basis
+ *                                  after glue (ligerito.rs:59-67)
+ *   "yr"                    steps  the final folded vector (prover.rs:104-110)
+ * *out receives the proof, as lg_prove. */
+typedef void (*lg_dump_cb)(void *user, const char *name, uint32_t level, const void *data, uint64_t bytes);
+lg_status lg_dump_intermediates(lg_ctx *ctx, const lg_config *cfg, const uint32_t *poly, uint64_t len,
+                                int poly_on_device, lg_dump_cb cb, void *user, lg_proof **out);
+
 /* verifier::<BinaryElem32>(config, proof), src/verifier.rs:10.  LG_OK with
  * *accepted = the reference's return value; LG_ERR_VERIFY_PANIC (accepted =
  * 0) where the reference panics (Merkle / Ligero asserts, malformed sizes). */

@@ -75,6 +75,11 @@ class LgConfig(ctypes.Structure):
     ]
 
 
+# lg_dump_cb: (user, name, level, data, bytes)
+_DUMP_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_void_p,
+                            ctypes.c_uint64)
+
+
 def _load() -> ctypes.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
@@ -108,6 +113,7 @@ def _load() -> ctypes.CDLL:
         "lg_device_table_bytes": (u64, [i32]),
         "lg_server_warm": (i32, [P, P, u32]),
         "lg_prove": (i32, [P, P, P, u64, i32, P]),
+        "lg_dump_intermediates": (i32, [P, P, P, u64, i32, _DUMP_CB, P, P]),
         "lg_verify": (i32, [P, P, P, P]),
         "lg_verify_bytes": (i32, [P, P, ctypes.c_char_p, u64, P]),
         "lg_proof_serialize": (i32, [P, P, P]),
@@ -593,6 +599,33 @@ def prover(config: ProverConfig, poly, ctx: Optional[Context] = None) -> Finaliz
         st = lib.lg_prove(ctx.handle, ctypes.byref(c), a.ctypes.data, a.size, 0, ctypes.byref(h))
     _check(st, ctx)
     return FinalizedLigeritoProof(h)
+
+
+def dump_intermediates(config: ProverConfig, poly, ctx: Optional[Context] = None):
+    """lg_dump_intermediates: the proof ``prover`` gives, plus a dict
+    {(name, level): bytes} of every intermediate the device produced on the
+    way (encoded matrices, Merkle trees, folded vectors, queries, opened
+    rows, induced bases, sumcheck triples, fold rounds, yr; the names and
+    levels are listed in include/ligerito_b200.h).  Synchronises at every
+    intermediate: a parity and debugging aid, not a fast path."""
+    ctx = ctx or default_context()
+    c = config.to_c()
+    got = {}
+
+    def cb(_user, name, level, data, nbytes):
+        got[(name.decode(), int(level))] = ctypes.string_at(data, nbytes)
+
+    fn = _DUMP_CB(cb)
+    h = ctypes.c_void_p()
+    if _is_torch(poly):
+        st = lib.lg_dump_intermediates(ctx.handle, ctypes.byref(c), _dev_ptr(poly), poly.numel(), 1, fn, None,
+                                       ctypes.byref(h))
+    else:
+        a = _u32(poly)
+        st = lib.lg_dump_intermediates(ctx.handle, ctypes.byref(c), a.ctypes.data, a.size, 0, fn, None,
+                                       ctypes.byref(h))
+    _check(st, ctx)
+    return FinalizedLigeritoProof(h), got
 
 
 def prove_lockstep(config: ProverConfig, polys, ctx: Optional[Context] = None) -> list:

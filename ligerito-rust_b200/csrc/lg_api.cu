@@ -61,6 +61,9 @@ struct lg_ctx {
     size_t pin_cap = 0, pin_used = 0, pin_want = 0;  // pin_want: the arena a call wanted
     uint8_t *dev_arena = nullptr;
     size_t dev_cap = 0, dev_used = 0;
+    // set only while lg_dump_intermediates runs
+    lg_dump_cb dump_cb = nullptr;
+    void *dump_user = nullptr;
 };
 
 namespace {
@@ -127,6 +130,19 @@ uint8_t *pinned(lg_ctx *c, size_t bytes) {
 }
 
 void sync(lg_ctx *c) { CK(c, cudaStreamSynchronize(c->stream)); }
+
+// lg_dump_intermediates: hand the caller a host copy of `bytes` device
+// bytes once the stream has produced them; nothing happens otherwise.
+void dump_dev(lg_ctx *c, const char *name, uint32_t level, const void *d, size_t bytes) {
+    if (!c->dump_cb) return;
+    std::vector<uint8_t> h(bytes);
+    sync(c);
+    CK(c, cudaMemcpy(h.data(), d, bytes, cudaMemcpyDeviceToHost));
+    c->dump_cb(c->dump_user, name, level, h.data(), bytes);
+}
+void dump_host(lg_ctx *c, const char *name, uint32_t level, const void *h, size_t bytes) {
+    if (c->dump_cb) c->dump_cb(c->dump_user, name, level, h, bytes);
+}
 
 void d2h(lg_ctx *c, void *dst, const void *src, size_t bytes) {
     uint8_t *p = pinned(c, bytes);
@@ -641,10 +657,28 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
         a.out = out;
         CK(c, lgk::fs_step(c->L, fs, a));
     };
+    // lg_dump_intermediates only (no-ops otherwise)
+    auto dump_commit = [&](uint32_t level, uint32_t log_m, const Witness &w) {
+        if (!c->dump_cb) return;
+        const Code code = get_code(c, log_m);
+        dump_dev(c, "twiddles", level, code.tw, 4 * ((4ull << log_m) - 1));
+        dump_dev(c, "pis", level, code.pis, 4ull << log_m);
+        dump_dev(c, "encoded", level, w.E.p, 4ull * w.rows * w.cols);
+        dump_dev(c, "tree", level, w.tree.p, 32ull * (2 * w.rows - 1));
+    };
+    auto dump_opening = [&](uint32_t level, const std::pair<const uint32_t *, const uint64_t *> &op, uint32_t cols,
+                            const uint32_t *d_alpha) {
+        dump_dev(c, "queries", level, op.second, 8ull * LG_NUM_QUERIES);
+        dump_dev(c, "opened_rows", level, op.first, 4ull * LG_NUM_QUERIES * cols);
+        dump_dev(c, "alpha", level, d_alpha, 4);
+    };
+    auto dump_triple = [&](const uint32_t *t) { dump_dev(c, "triple", (uint32_t)((t - tri) / 4), t, 12); };
+    uint32_t round_no = 0;
 
     Witness w0 = h_poly ? commit_from_host(c, sc, h_poly, const_cast<uint32_t *>(d_poly), cfg.initial_log_m,
                                            1u << cfg.initial_log_n)
                         : commit(c, d_poly, cfg.initial_log_m, 1u << cfg.initial_log_n);  // :32-37
+    dump_commit(0, cfg.initial_log_m, w0);
     uint32_t *root_m = root_later(&P.initial_root);
     P.recursive_roots.resize(steps);
     P.recursive.resize(steps - 1);  // openings are filled in by pointer later
@@ -653,8 +687,11 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
     uint32_t fv = cfg.initial_log_m;  // log2 |f|
     DBuf f(c, 4ull << fv);
     partial_eval_dev(c, d_poly, cfg.initial_log_m + cfg.initial_log_n, nullptr, cfg.initial_k, f.u32(), pe0);  // :52-53
+    dump_dev(c, "fold_challenges", 0, pe0, 4ull * cfg.initial_k);
+    dump_dev(c, "folded", 0, f.p, 4ull << fv);
 
     Witness wprev = commit(c, f.u32(), cfg.log_m[0], 1u << cfg.log_n[0]);  // :55-60
+    dump_commit(1, cfg.log_m[0], wprev);
     root_m = root_later(&P.recursive_roots[0]);
     uint32_t *alpha = next_chal(1);
     auto opened = open_rows_dev(c, sc, w0, fs, wprev.root(), 1, alpha, &P.initial, root_m);  // :64-76
@@ -662,6 +699,9 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
     uint32_t *t = next_tri();
     induce_dev(c, sc, fv, opened.first, LG_NUM_QUERIES, nullptr, cfg.initial_k, opened.second, 0, B.u32(), t + 3, pe0,
                alpha);  // :78-85
+    dump_opening(0, opened, w0.cols, alpha);
+    dump_dev(c, "basis", 0, B.p, 4ull << fv);
+    dump_dev(c, "enforced_sum", 0, t + 3, 4);
     w0.E.reset();
     w0.tree.reset();
     uint32_t *r = next_chal(1);
@@ -669,6 +709,7 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
     // first challenge of :97
     const lgk::FsTail t0 = tail(true, 1, r);
     CK(c, lgk::eval013(c->L, f.u32(), B.u32(), fv, t, &t0));
+    dump_triple(t);
 
     DBuf f2(c, 4ull << (fv - 1)), B2(c, 4ull << (fv - 1));
     for (uint32_t i = 0; i < steps; ++i) {
@@ -700,6 +741,13 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
             std::swap(f, f2);
             std::swap(B, B2);
             fv -= 1;
+            if (c->dump_cb) {
+                dump_dev(c, "round_challenge", round_no, r, 4);
+                dump_dev(c, "round_f", round_no, f.p, 4ull << fv);
+                dump_dev(c, "round_basis", round_no, B.p, 4ull << fv);
+                dump_triple(t);
+            }
+            ++round_no;
             r = rn;
         }
         if (i == steps - 1) {  // :104-143
@@ -725,24 +773,33 @@ void prove_impl(lg_ctx *c, Scratch &sc, const lg_config &cfg, const uint32_t *d_
             fsh.absorb_u32s(P.yr.data(), P.yr.size());
             std::vector<uint64_t> q;
             if (!fsh.get_distinct_queries(wprev.rows, LG_NUM_QUERIES, q)) throw ProverAssert{};
+            dump_host(c, "yr", steps, P.yr.data(), 4 * P.yr.size());
+            dump_host(c, "queries", steps, q.data(), 8 * q.size());
             if (h_E) open_rows_host(h_E, h_tree, wprev.rows, wprev.cols, q, &P.final_);
             else open_rows(c, sc, wprev, q, &P.final_);
             return;
         }
         Witness wn = commit(c, f.u32(), cfg.log_m[i + 1], 1u << cfg.log_n[i + 1]);  // :145-155
+        dump_commit(i + 2, cfg.log_m[i + 1], wn);
         root_m = root_later(&P.recursive_roots[i + 1]);
         uint32_t *al = next_chal(1);
         auto op = open_rows_dev(c, sc, wprev, fs, wn.root(), 1, al, &P.recursive[i], root_m);  // :156-172
         DBuf bi(c, 4ull << fv);
         t = next_tri();
         induce_dev(c, sc, fv, op.first, LG_NUM_QUERIES, nullptr, cfg.ks[i], op.second, 0, bi.u32(), t + 3, rs, al);
+        dump_opening(i + 1, op, wprev.cols, al);
+        dump_dev(c, "basis", i + 1, bi.p, 4ull << fv);
+        dump_dev(c, "enforced_sum", i + 1, t + 3, 4);
         // introduce_new, :187-193 (src/ligerito.rs:52): the glue challenge,
         // then the next step's first round challenge
         uint32_t *beta = next_chal(2);
         const lgk::FsTail ti = tail(true, 2, beta);
         CK(c, lgk::eval013(c->L, f.u32(), bi.u32(), fv, t, &ti));
+        dump_triple(t);
         r = beta + 1;
         CK(c, lgk::axpy(c->L, B.u32(), bi.u32(), fv, 0, beta));  // glue
+        dump_dev(c, "beta", i + 1, beta, 4);
+        dump_dev(c, "basis_sum", i + 1, B.p, 4ull << fv);
         wprev = std::move(wn);
     }
     throw ProverAssert{};  // :198
@@ -1725,6 +1782,18 @@ lg_status lg_prove(lg_ctx *c, const lg_config *cfg, const uint32_t *poly, uint64
     if (st != LG_OK) { delete res; return st; }
     *out = res;
     return LG_OK;
+}
+
+lg_status lg_dump_intermediates(lg_ctx *c, const lg_config *cfg, const uint32_t *poly, uint64_t len, int on_device,
+                                lg_dump_cb cb, void *user, lg_proof **out) {
+    if (!c || !cb) return LG_ERR_INVALID_ARGUMENT;
+    struct Hook {  // cleared however lg_prove returns
+        lg_ctx *c;
+        ~Hook() { c->dump_cb = nullptr; c->dump_user = nullptr; }
+    } hook{c};
+    c->dump_cb = cb;
+    c->dump_user = user;
+    return lg_prove(c, cfg, poly, len, on_device, out);
 }
 
 lg_status lg_prove_lockstep(lg_ctx *c, const lg_config *cfg, const uint32_t *const *polys, uint64_t len,
