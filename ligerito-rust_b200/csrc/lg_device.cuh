@@ -96,19 +96,76 @@ __device__ __forceinline__ U128 gf128_mul(U128 a, U128 b) {
 // 4-bit windows: 8 windows x 16 entries = 128 words (512 B) per constant.
 constexpr int kTabWords = 128;
 
-// One warp builds the table of constant c (all 32 lanes participate).
+// Table builds run their carry-less products on the multiply-add pipe,
+// which the table kernels otherwise leave idle: an integer product t * k
+// equals the carry-less one when the shifted copies of t that k's set bits
+// make never overlap.  The multipliers come from constant memory so the
+// compiler keeps them multiplies.
+static __constant__ uint32_t kTabMul[9] = {
+    256u,     // v x^8 (the low word)
+    0x201u,   // t (1 + x^9), t < 2^8
+    0x8080u,  // t (x^7 + x^15), t < 2^8
+    8u,       // t x^3
+    16u,      // t x^4, and v x^4 (the low word)
+    0x8211u,  // t (1 + x^4 + x^9 + x^15), t < 2^4
+    0x88u,    // t (x^3 + x^7), t < 2^4
+    0x8089u,  // t (1 + x^3 + x^7 + x^15), t < 2^3
+    0x210u,   // t (x^4 + x^9), t < 2^3
+};
+__device__ __forceinline__ uint32_t fma_mul(uint32_t a, uint32_t k) {
+    uint32_t r;
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(k));
+    return r;
+}
+__device__ __forceinline__ uint64_t fma_mul_wide(uint32_t a, uint32_t k) {
+    uint64_t r;
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(r) : "r"(a), "r"(k));
+    return r;
+}
+// v x^8 mod p: (v << 8) ^ t (x^15 + x^9 + x^7 + x^4 + x^3 + 1), t = v >> 24,
+// the tail split into the non-overlapping shift sets {0, 9}, {7, 15}, {3}, {4}
+__device__ __forceinline__ uint32_t tab_mulx8(uint32_t v) {
+    const uint32_t t = v >> 24;
+    return fma_mul(v, kTabMul[0]) ^ fma_mul(t, kTabMul[1]) ^ fma_mul(t, kTabMul[2]) ^ fma_mul(t, kTabMul[3]) ^
+           fma_mul(t, kTabMul[4]);
+}
+
+// One warp builds the table of constant c (all 32 lanes participate): lane
+// l writes entries l, 32 + l, 64 + l, 96 + l, i.e. c e x^(4w) for e = l & 15
+// and windows w = 2j + (l >> 4), j < 4.  c e is a carry-less product by a
+// 4-bit e: c's bits taken every 4th (four masks) times e never carry, so it
+// is four wide integer products XORed; the at most 3 bits past x^31 fold
+// back through the tail.  Lanes 16-31 start from c x^4; each next pair of
+// windows is a multiplication by x^8.
+__device__ __forceinline__ void tab_entries(uint32_t c, int lane, uint32_t (&v)[4]) {
+    const uint32_t t4 = c >> 28;
+    const uint32_t c4 = fma_mul(c, kTabMul[4]) ^ fma_mul(t4, kTabMul[5]) ^ fma_mul(t4, kTabMul[6]);
+    const uint32_t cs = (lane & 16) ? c4 : c, e = lane & 15;
+    const uint64_t p = fma_mul_wide(cs & 0x11111111u, e) ^ fma_mul_wide(cs & 0x22222222u, e) ^
+                       fma_mul_wide(cs & 0x44444444u, e) ^ fma_mul_wide(cs & 0x88888888u, e);
+    const uint32_t hi = (uint32_t)(p >> 32);
+    v[0] = (uint32_t)p ^ fma_mul(hi, kTabMul[7]) ^ fma_mul(hi, kTabMul[8]);
+    v[1] = tab_mulx8(v[0]);
+    v[2] = tab_mulx8(v[1]);
+    v[3] = tab_mulx8(v[2]);
+}
 __device__ __forceinline__ void tab_build_warp(uint32_t *T, uint32_t c, int lane) {
-    uint32_t c1 = gf_mulx(c), c2 = gf_mulx(c1), c3 = gf_mulx(c2);
-    int e = lane & 15;
-    uint32_t v = ((e & 1) ? c : 0u) ^ ((e & 2) ? c1 : 0u) ^ ((e & 4) ? c2 : 0u) ^ ((e & 8) ? c3 : 0u);
-    if (lane & 16) v = gf_mulxk<4>(v);
-    T[lane] = v;
-    v = gf_mulxk<8>(v);
-    T[32 + lane] = v;
-    v = gf_mulxk<8>(v);
-    T[64 + lane] = v;
-    v = gf_mulxk<8>(v);
-    T[96 + lane] = v;
+    uint32_t v[4];
+    tab_entries(c, lane, v);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) T[32 * j + lane] = v[j];
+}
+// The tables of two constants interleaved: entry (w, e) = (c0 e x^(4w),
+// c1 e x^(4w)) in 8 bytes at byte 128 w + 8 e (1 KB a pair).  For values
+// multiplied by both constants (tab2_mul_sa) the nibble spreads and byte
+// permutes are paid once and each window is one 64-bit load; a half-warp
+// reads 16 distinct entries of a 128-byte window, conflict-free.
+__device__ __forceinline__ void tab2_build_warp(uint2 *T, uint32_t c0, uint32_t c1, int lane) {
+    uint32_t v0[4], v1[4];
+    tab_entries(c0, lane, v0);
+    tab_entries(c1, lane, v1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) T[32 * j + lane] = make_uint2(v0[j], v1[j]);
 }
 
 // Same product with the table at byte offset base + off of the shared
@@ -151,6 +208,25 @@ __device__ __forceinline__ uint32_t tab_mul_sa(const uint8_t *__restrict__ sm, u
     const uint32_t r6 = LGD_LD(a, 0x7653, 384), r7 = LGD_LD(b, 0x7653, 448);
 #undef LGD_LD
     return (r0 ^ r1 ^ r2) ^ (r3 ^ r4 ^ r5) ^ (r6 ^ r7);
+}
+// w times both constants of the pair table at byte offset base of `sm`
+// (base a multiple of 256): byte j of a (b) holds 8 * nibble 2j (2j+1) of
+// w, the byte offset of that window's 8-byte entry.
+static __constant__ uint32_t kSpreadMul2[2] = {8u, 1u << 31};
+__device__ __forceinline__ uint2 tab2_mul_sa(const uint8_t *__restrict__ sm, uint32_t base, uint32_t w) {
+    uint32_t a, b;
+    asm("mul.lo.u32 %0, %1, %2;" : "=r"(a) : "r"(w), "r"(kSpreadMul2[0]));
+    asm("mul.hi.u32 %0, %1, %2;" : "=r"(b) : "r"(w), "r"(kSpreadMul2[1]));
+    a &= 0x78787878u;
+    b &= 0x78787878u;
+#define LGD_LD2(x, sel, o) (*reinterpret_cast<const uint2 *>(sm + __byte_perm((x), base, (sel)) + (o)))
+    const uint2 r0 = LGD_LD2(a, 0x7650, 0), r1 = LGD_LD2(b, 0x7650, 128);
+    const uint2 r2 = LGD_LD2(a, 0x7651, 256), r3 = LGD_LD2(b, 0x7651, 384);
+    const uint2 r4 = LGD_LD2(a, 0x7652, 512), r5 = LGD_LD2(b, 0x7652, 640);
+    const uint2 r6 = LGD_LD2(a, 0x7653, 768), r7 = LGD_LD2(b, 0x7653, 896);
+#undef LGD_LD2
+    return make_uint2((r0.x ^ r1.x ^ r2.x) ^ (r3.x ^ r4.x ^ r5.x) ^ (r6.x ^ r7.x),
+                      (r0.y ^ r1.y ^ r2.y) ^ (r3.y ^ r4.y ^ r5.y) ^ (r6.y ^ r7.y));
 }
 
 // ---------------------------------------------------------------- BLAKE3

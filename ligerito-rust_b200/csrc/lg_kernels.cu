@@ -114,7 +114,7 @@ __global__ void k_rs_scale(const uint32_t *__restrict__ poly, const uint32_t *__
 constexpr uint32_t kScaleRows = 32, kScaleCols = 64, kScaleThreads = 256;
 static_assert(kScaleCols == 64 && kScaleRows % (kScaleThreads / 32) == 0, "two column halves per lane");
 constexpr uint32_t kScalePer = kScaleRows * kScaleCols / kScaleThreads;  // words per thread
-__global__ void __launch_bounds__(kScaleThreads) k_rs_scale_tab(const uint32_t *__restrict__ poly,
+__global__ void __launch_bounds__(kScaleThreads, 4) k_rs_scale_tab(const uint32_t *__restrict__ poly,
                                                                 const uint32_t *__restrict__ pis,
                                                                 uint32_t *__restrict__ out, uint32_t log_m, uint32_t n) {
     pdl_begin();
@@ -1501,6 +1501,73 @@ __global__ void __launch_bounds__(256, ACC <= 16 ? 3 : 2) k_induce_main(const ui
     }
 }
 
+// The same basis when 2^(n-b) >= 2 (n > 9, so 2^b = 512 and ACC = 16):
+// work items are (proof, pair of t_hi, query) triples, and each warp builds
+// the interleaved table of (Hi_k[2 t], Hi_k[2 t + 1]) and multiplies each
+// Lo_k word by both with one lookup per window (tab2_mul_sa), so the two
+// output rows 2t and 2t + 1 share every nibble spread, permute and load
+// instruction.
+__global__ void __launch_bounds__(256, 2) k_induce_main2(const uint32_t *__restrict__ lo, const uint32_t *__restrict__ hi,
+                                                      uint32_t n, uint32_t nq, uint32_t B, uint32_t *__restrict__ out,
+                                                      InduceStrides st) {
+    pdl_begin();
+    constexpr int ACC = 16;
+    constexpr uint32_t nlo = 32 * ACC;  // b = 9
+    __shared__ __align__(256) uint2 tabs[8][kTabWords];
+    __shared__ uint32_t red[2 * nlo];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t nhi = 1u << (n - 9), npair = nhi / 2;
+    const uint64_t P = (uint64_t)B * npair * nq;
+    uint64_t p = blockIdx.x * P / gridDim.x;
+    const uint64_t pend = (blockIdx.x + 1) * P / gridDim.x;
+    const uint8_t *tab8 = reinterpret_cast<const uint8_t *>(tabs);
+    while (p < pend) {
+        const uint64_t seg = p / nq;
+        const uint32_t k0 = (uint32_t)(p - seg * nq);
+        const uint64_t left = pend - p;
+        const uint32_t k1 = left < (uint64_t)(nq - k0) ? k0 + (uint32_t)left : nq;
+        const uint32_t pb = (uint32_t)(seg / npair), tp = (uint32_t)(seg - (uint64_t)pb * npair);
+        const uint32_t *lop = lo + pb * st.lo, *hip = hi + pb * st.hi;
+        uint32_t acc0[ACC], acc1[ACC];
+#pragma unroll
+        for (int c = 0; c < ACC; ++c) acc0[c] = acc1[c] = 0;
+        // the query's Lo words are loaded (from L2) before the warp builds
+        // its table, so their latency passes under the build
+        for (uint32_t k = k0 + warp; k < k1; k += nw) {
+            const uint32_t *lk = lop + (uint64_t)k * nlo + lane;
+            uint32_t v[ACC];
+#pragma unroll
+            for (int c = 0; c < ACC; ++c) v[c] = __ldg(lk + 32 * c);
+            const uint2 h = __ldg(reinterpret_cast<const uint2 *>(hip + (uint64_t)k * nhi) + tp);
+            tab2_build_warp(tabs[warp], h.x, h.y, lane);
+            __syncwarp();
+#pragma unroll
+            for (int c = 0; c < ACC; ++c) {
+                const uint2 r = tab2_mul_sa(tab8, 1024u * warp, v[c]);
+                acc0[c] ^= r.x;
+                acc1[c] ^= r.y;
+            }
+            __syncwarp();
+        }
+        for (uint32_t w = threadIdx.x; w < 2 * nlo; w += blockDim.x) red[w] = 0;
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < ACC; ++c) {
+            atomicXor(&red[lane + 32 * c], acc0[c]);
+            atomicXor(&red[nlo + lane + 32 * c], acc1[c]);
+        }
+        __syncthreads();
+        uint32_t *dst = out + pb * st.out + (uint64_t)(2 * tp) * nlo;  // rows 2tp and 2tp + 1
+        const bool whole = k0 == 0 && k1 == nq;
+        for (uint32_t w = threadIdx.x; w < 2 * nlo; w += blockDim.x) {
+            if (whole) dst[w] = red[w];
+            else atomicXor(dst + w, red[w]);
+        }
+        __syncthreads();  // red is reused by the next segment
+        p += k1 - k0;
+    }
+}
+
 // One wave of induce_main blocks (occupancy of the instantiation, cached).
 template <int ACC>
 static unsigned induce_grid(uint64_t work) {
@@ -1534,6 +1601,21 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
     if (e != cudaSuccess) return e;
     const uint64_t work = (uint64_t)B * (1ull << (n - p.b)) * nq;
     L.note(4.0 * B * (vec + (1ull << n)), (double)B * nq * (1ull << n));
+    if (p.b == 9 && n > 9) {
+        static std::atomic<int> occ2{0};
+        int o = occ2.load(std::memory_order_relaxed);
+        if (!o) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_induce_main2, 256, 0) != cudaSuccess || o < 1) o = 1;
+            occ2.store(o, std::memory_order_relaxed);
+        }
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+        // at least 32 (proof, t_hi pair, query) triples a block
+        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((work / 2 + 31) / 32, (uint64_t)sms * o));
+        LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main2, grid, 256, 0, L.stream, d_lo, d_hi, n, nq, B, out, st));
+        return cudaGetLastError();
+    }
     switch (std::max<uint32_t>(1, (1u << p.b) / 32)) {
 #define LGK_CASE(a) \
     case a: LGK_LAUNCH(L, "induce_main", launch_k(k_induce_main<a>, induce_grid<a>(work), 256, 0, L.stream, d_lo, d_hi, n, p.b, nq, B, out, st)); break;
