@@ -275,7 +275,15 @@ __device__ void store_state(const FsState &S, FsState *g) {
 // last one reads the total, checks it against the enforced sum acc3[3] when
 // asked, absorbs it and squeezes t.nsq challenges.  No block waits: a block
 // that is not last returns.
-__device__ void fs_tail_block(const FsTail &t, uint32_t *acc3) {
+// Every block reads the transcript state at its start (fs_tail_prefetch,
+// one word per thread; nothing writes it before the last block does), so
+// the last block does not wait for that read after learning it is last.
+constexpr uint32_t kFsStateWords = sizeof(FsState) / 4;
+static_assert(kFsStateWords <= 64, "the state is prefetched by the first threads of a block");
+__device__ __forceinline__ uint32_t fs_tail_prefetch(const FsTail &t) {
+    return t.fs && threadIdx.x < kFsStateWords ? reinterpret_cast<const uint32_t *>(t.fs)[threadIdx.x] : 0u;
+}
+__device__ void fs_tail_block(const FsTail &t, uint32_t *acc3, uint32_t pre) {
     __shared__ FsState S;
     __shared__ Batch B;
     __shared__ uint32_t tri[4];
@@ -287,7 +295,8 @@ __device__ void fs_tail_block(const FsTail &t, uint32_t *acc3) {
     if (!last) return;
     __threadfence();
     if (threadIdx.x < 4) tri[threadIdx.x] = atomicOr(acc3 + threadIdx.x, 0u);
-    load_state(S, t.fs);
+    if (threadIdx.x < kFsStateWords) reinterpret_cast<uint32_t *>(&S)[threadIdx.x] = pre;
+    __syncthreads();
     if (threadIdx.x == 0) {
         if (t.check && (tri[0] ^ tri[1]) != tri[3]) S.err |= FS_ERR_SUMCHECK;
         fs_absorb(S, tri, 3);

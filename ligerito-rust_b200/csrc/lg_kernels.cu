@@ -1184,6 +1184,7 @@ __global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__rest
     g += b * st.g;
     acc3 += b * st.acc;
     tail = tail_for(tail, st, b);
+    const uint32_t fs_pre = fsd::fs_tail_prefetch(tail);
     uint32_t s0 = 0, s1 = 0, s2 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t f0 = f[i], f1 = f[half + i], g0 = g[i], g1 = g[half + i];
@@ -1192,7 +1193,7 @@ __global__ void k_eval013(const uint32_t *__restrict__ f, const uint32_t *__rest
         s2 ^= gf_mul(at3(f0, f1), at3(g0, g1));
     }
     block_xor3(s0, s1, s2, acc3);
-    if (tail.fs) fsd::fs_tail_block(tail, acc3);
+    if (tail.fs) fsd::fs_tail_block(tail, acc3, fs_pre);
 }
 cudaError_t eval013(Launcher &L, const uint32_t *f, const uint32_t *g, uint32_t log_len, uint32_t *acc3,
                     const FsTail *tail, uint32_t B, const RoundStrides &st) {
@@ -1224,13 +1225,25 @@ __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__
         tail = tail_for(tail, st, b);
     }
     __shared__ __align__(128) uint32_t T[kTabWords];
+    // the thread's first words are loaded before the challenge's table is
+    // built, so the two memory latencies overlap; each later iteration's
+    // words load while the current one is multiplied
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint32_t v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    auto load = [&](uint64_t j) {
+        v[0] = f[j]; v[1] = f[quarter + j]; v[2] = f[2 * quarter + j]; v[3] = f[3 * quarter + j];
+        v[4] = B[j]; v[5] = B[quarter + j]; v[6] = B[2 * quarter + j]; v[7] = B[3 * quarter + j];
+    };
+    if (i < quarter) load(i);
+    const uint32_t fs_pre = fsd::fs_tail_prefetch(tail);
     if (threadIdx.x < 32) tab_build_warp(T, d_r ? *d_r : r, threadIdx.x);
     __syncthreads();
     const uint8_t *t8 = reinterpret_cast<const uint8_t *>(T);
     uint32_t s0 = 0, s1 = 0, s2 = 0;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < quarter; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t a0 = f[i], a1 = f[quarter + i], a2 = f[2 * quarter + i], a3 = f[3 * quarter + i];
-        const uint32_t c0 = B[i], c1 = B[quarter + i], c2 = B[2 * quarter + i], c3 = B[3 * quarter + i];
+    for (; i < quarter; i += stride) {
+        const uint32_t a0 = v[0], a1 = v[1], a2 = v[2], a3 = v[3], c0 = v[4], c1 = v[5], c2 = v[6], c3 = v[7];
+        if (i + stride < quarter) load(i + stride);
         const uint32_t flo = a0 ^ tab_mul_sa(t8, 0, 0, a0 ^ a2), fhi = a1 ^ tab_mul_sa(t8, 0, 0, a1 ^ a3);
         const uint32_t blo = c0 ^ tab_mul_sa(t8, 0, 0, c0 ^ c2), bhi = c1 ^ tab_mul_sa(t8, 0, 0, c1 ^ c3);
         fo[i] = flo; fo[quarter + i] = fhi;
@@ -1240,7 +1253,7 @@ __global__ void __launch_bounds__(256) k_fold_round(const uint32_t *__restrict__
         s2 ^= gf_mul(at3(flo, fhi), at3(blo, bhi));
     }
     block_xor3(s0, s1, s2, acc3);
-    if (tail.fs) fsd::fs_tail_block(tail, acc3);
+    if (tail.fs) fsd::fs_tail_block(tail, acc3, fs_pre);
 }
 cudaError_t fold_round(Launcher &L, const uint32_t *f, const uint32_t *B, uint32_t log_len, uint32_t r,
                        uint32_t *fo, uint32_t *Bo, uint32_t *acc3, const uint32_t *d_r, const FsTail *tail,
@@ -1262,10 +1275,18 @@ __global__ void k_axpy(uint32_t *__restrict__ B, const uint32_t *__restrict__ bi
     bi += blockIdx.y * st.g;
     if (d_beta) d_beta += blockIdx.y * st.r;
     __shared__ __align__(128) uint32_t T[kTabWords];
+    // the first words load before the table is built (their latencies overlap)
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint32_t b0 = 0, x0 = 0;
+    if (i < n) { b0 = B[i]; x0 = bi[i]; }
     if (threadIdx.x < 32) tab_build_warp(T, d_beta ? *d_beta : beta, threadIdx.x);
     __syncthreads();
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        B[i] ^= tab_mul_sa(reinterpret_cast<const uint8_t *>(T), 0, 0, bi[i]);
+    for (; i < n; i += stride) {
+        const uint32_t b = b0, x = x0;
+        if (i + stride < n) { b0 = B[i + stride]; x0 = bi[i + stride]; }
+        B[i] = b ^ tab_mul_sa(reinterpret_cast<const uint8_t *>(T), 0, 0, x);
+    }
 }
 cudaError_t axpy(Launcher &L, uint32_t *B, const uint32_t *bi, uint32_t log_len, uint32_t beta,
                  const uint32_t *d_beta, uint32_t NB, const RoundStrides &st) {
