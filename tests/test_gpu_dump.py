@@ -123,3 +123,21 @@ def test_intermediates_match_oracle(lg, ref, ctx, golden, name):
             got.append(int(u32(d[("beta", lv)])[0]))
         got += step_rounds[lv]
     assert got == ch
+
+
+def test_dump_hook_is_cleared_and_checks_arguments(lg, ctx, golden):
+    # a dump leaves the context as it was: the next plain proof gives the
+    # same bytes and calls no callback; a missing callback is refused
+    case = golden["cases"]["small_L12"]
+    steps, m0, n0, k0, lms, lns, ks = case["config"]
+    pc = lg.ProverConfig(steps, (1 << m0, 1 << n0), [(1 << m, 1 << n) for m, n in zip(lms, lns)], k0, list(ks))
+    poly = lg.to_device(lg.splitmix_coeffs(case["seed"], pc.poly_len))
+    dumped, d = lg.dump_intermediates(pc, poly, ctx)
+    assert len(d) > 10
+    assert lg.prover(pc, poly, ctx).to_bytes() == dumped.to_bytes()
+    import ctypes
+
+    h = ctypes.c_void_p()
+    st = lg.lib.lg_dump_intermediates(ctx.handle, ctypes.byref(pc.to_c()), lg._dev_ptr(poly), poly.numel(), 1,
+                                      ctypes.cast(None, lg._DUMP_CB), None, ctypes.byref(h))
+    assert lg.STATUS[st] == "invalid argument"
