@@ -354,18 +354,30 @@ Witness commit(lg_ctx *c, const uint32_t *d_poly, uint32_t log_m, uint32_t n) {
     return w;
 }
 
+// Hash units of the host-input commitment: 32 columns (two BLAKE3 blocks of
+// every leaf) when there are at least 64, else 16 (one block).  The last
+// FFT pass runs once per unit, and its table work per tile does not shrink
+// with the columns, so a 16-column unit costs about as much GPU time per
+// column as its copy takes and the compute falls behind the copy; 32
+// keeps it ahead.
+uint32_t host_hash_unit(uint32_t n) { return n >= 64 ? 32 : std::min<uint32_t>(16, n); }
+
 // Copy groups of the host-input commitment (column counts, in order): the
-// columns form hash units of 16 (one BLAKE3 block of every leaf); the
-// first unit arrives as 1/4, 1/4, 1/2 of it so that compute starts after
-// a few columns, the last as two halves so that little work remains after
-// the last bytes land, the units between whole.
+// first unit arrives as 1/8, 1/8, 1/4, 1/2 of it (a 16-column unit as 1/4,
+// 1/4, 1/2) so that compute starts after a few columns, the last as 1/2,
+// 1/4, 1/4 (a 16-column unit as two halves) so that little work remains
+// after the last bytes land, the units between whole.
 std::vector<uint32_t> host_copy_groups(uint32_t n) {
-    const uint32_t U = std::min<uint32_t>(16, n), units = (n + U - 1) / U;
+    const uint32_t U = host_hash_unit(n), units = (n + U - 1) / U;
     std::vector<uint32_t> g;
     for (uint32_t u = 0; u < units; ++u) {
         const uint32_t cols = std::min(U, n - u * U);
-        if (u == 0 && cols >= 8 && cols % 4 == 0) {
+        if (u == 0 && cols == 32) {
+            g.insert(g.end(), {4, 4, 8, 16});
+        } else if (u == 0 && cols >= 8 && cols % 4 == 0) {
             g.insert(g.end(), {cols / 4, cols / 4, cols / 2});
+        } else if (u + 1 == units && cols == 32) {
+            g.insert(g.end(), {16, 8, 8});
         } else if (u + 1 == units && cols >= 8 && cols % 2 == 0) {
             g.insert(g.end(), {cols / 2, cols / 2});
         } else {
@@ -379,11 +391,12 @@ std::vector<uint32_t> host_copy_groups(uint32_t n) {
 // columns travel in groups (host_copy_groups) on the copy stream; the
 // compute stream waits for each group and, while the next is in flight,
 // runs its scale-and-spread and the FFT passes but the last (columns are
-// independent).  Each hash unit of 16 columns, once all its groups are
-// in, gets the last FFT pass and its BLAKE3 block of every leaf: a leaf is
+// independent).  Each hash unit (host_hash_unit), once all its groups are
+// in, gets the last FFT pass and its BLAKE3 blocks of every leaf: a leaf is
 // the row's words in column order and 16 words are one BLAKE3 block, so
-// unit u is block u of each leaf's chunk, chained through the leaf slots
-// of the tree.  After the last unit only the upper tree remains.
+// columns 16b .. 16b+15 are block b of each leaf's chunk, chained through
+// the leaf slots of the tree.  After the last unit only the upper tree
+// remains.
 Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_t *d_poly, uint32_t log_m,
                          uint32_t n) {
     const Code code = get_code(c, log_m);
@@ -397,7 +410,7 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
     const bool pinned_src = cudaPointerGetAttributes(&attr, h_poly) == cudaSuccess && attr.type == cudaMemoryTypeHost;
     cudaGetLastError();
     const std::vector<uint32_t> groups = host_copy_groups(n);
-    const uint32_t U = std::min<uint32_t>(16, n);
+    const uint32_t U = host_hash_unit(n);
     DBuf scaled(c, log_m > 6 ? 4ull * n * m : 0);
     // staging for pageable input: two pinned chunks, reused after their copy
     constexpr size_t kChunk = 4u << 20;
@@ -439,7 +452,9 @@ Witness commit_from_host(lg_ctx *c, Scratch &sc, const uint32_t *h_poly, uint32_
             const uint32_t u = (j0 - 1) / U, ju = u * U, ucols = j0 - ju;
             CK(c, lgk::fft_vectors(c->L, w.E.u32() + (uint64_t)ju * rows, code.tw, log_m, ucols, rows, 4, m, 4, false,
                                    lgk::FFT_LAST));
-            CK(c, lgk::leaf_hash_block(c->L, w.E.u32(), rows, n, u, 1, w.tree.u32()));
+            // the unit's BLAKE3 blocks of every leaf, chained after the earlier units'
+            const uint32_t b0 = ju / 16, nb = (ucols + 15) / 16;
+            CK(c, lgk::leaf_hash_block(c->L, w.E.u32(), rows, n, b0, nb, w.tree.u32()));
         }
     }
     CK(c, lgk::merkle_upper(c->L, w.tree.u32(), rows));
