@@ -564,10 +564,9 @@ void induce_dev(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *d_rows, uint
     uint32_t *d_apow = static_cast<uint32_t *>(sc.dev(8ull * nq));
     uint32_t *d_lo = static_cast<uint32_t *>(sc.dev(4ull * nq << plan.b));
     uint32_t *d_hi = static_cast<uint32_t *>(sc.dev(4ull * nq << (n - plan.b)));
-    CK(c, lgk::induce_setup(c->L, d_rows, 1u << nch, d_vch ? nullptr : gr.data(), d_q, nq, alpha, n, sks.data(), d_S,
-                            d_apow, d_vch, d_alpha));
     if (plan.needs_zero) CK(c, cudaMemsetAsync(d_out, 0, 4ull << n, c->stream));
-    CK(c, lgk::induce_basis(c->L, plan, d_S, d_apow, n, nq, d_lo, d_hi, d_out, d_sum));
+    CK(c, lgk::induce_fused(c->L, plan, d_rows, 1u << nch, d_vch ? nullptr : gr.data(), d_q, nq, alpha, n,
+                            sks.data(), d_S, d_apow, d_vch, d_alpha, d_lo, d_hi, d_out, d_sum));
 }
 
 // host rows / queries (verifier, kernel-level API) -> induce_dev
@@ -943,10 +942,9 @@ void induce_batch(lg_ctx *c, Scratch &sc, uint32_t n, const uint32_t *d_rows, ui
     uint32_t *d_apow = static_cast<uint32_t *>(sc.dev(4ull * st.apow * B));
     uint32_t *d_lo = static_cast<uint32_t *>(sc.dev(4ull * st.lo * B));
     uint32_t *d_hi = static_cast<uint32_t *>(sc.dev(4ull * st.hi * B));
-    CK(c, lgk::induce_setup(c->L, d_rows, 1u << nch, nullptr, d_q, nq, 0, n, sks.data(), d_S, d_apow, d_vch, d_alpha,
-                            B, st));
     if (plan.needs_zero) CK(c, cudaMemsetAsync(d_out, 0, (4ull << n) * B, c->stream));
-    CK(c, lgk::induce_basis(c->L, plan, d_S, d_apow, n, nq, d_lo, d_hi, d_out, d_sum, B, st));
+    CK(c, lgk::induce_fused(c->L, plan, d_rows, 1u << nch, nullptr, d_q, nq, 0, n, sks.data(), d_S, d_apow, d_vch,
+                            d_alpha, d_lo, d_hi, d_out, d_sum, B, st));
 }
 
 // partial_eval_dev for the B proofs (inputs in_stride apart, outputs and

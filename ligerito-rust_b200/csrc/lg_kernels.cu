@@ -1608,6 +1608,8 @@ static unsigned induce_grid(uint64_t work) {
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((work + 31) / 32, (uint64_t)sms * o));
 }
 
+static cudaError_t launch_induce_main(Launcher &L, const InducePlan &p, uint32_t n, uint32_t nq, const uint32_t *d_lo,
+                                      const uint32_t *d_hi, uint32_t *out, uint32_t B, const InduceStrides &st);
 cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, const uint32_t *d_apow,
                          uint32_t n, uint32_t nq, uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum,
                          uint32_t B, const InduceStrides &st) {
@@ -1620,6 +1622,13 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
                                           d_apow, n, p.b, nq, d_lo, d_hi, d_sum, in_smem, out, st));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    return launch_induce_main(L, p, n, nq, d_lo, d_hi, out, B, st);
+}
+
+// induce_main (pair tables when 2^(n-b) >= 2) over Lo / Hi from the prep
+static cudaError_t launch_induce_main(Launcher &L, const InducePlan &p, uint32_t n, uint32_t nq, const uint32_t *d_lo,
+                                      const uint32_t *d_hi, uint32_t *out, uint32_t B, const InduceStrides &st) {
+    const double vec = (double)nq * ((1ull << p.b) + (1ull << (n - p.b)));
     const uint64_t work = (uint64_t)B * (1ull << (n - p.b)) * nq;
     L.note(4.0 * B * (vec + (1ull << n)), (double)B * nq * (1ull << n));
     if (p.b == 9 && n > 9) {
@@ -1645,6 +1654,133 @@ cudaError_t induce_basis(Launcher &L, const InducePlan &p, const uint32_t *d_S, 
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+// induce_setup and induce_prep in one launch: block k (query k) first
+// runs the setup of its query on warp 0 (the row's dot product with the
+// Lagrange basis, alpha^k, the subspace values) into shared memory, then
+// the block doubles out Lo_k and Hi_k from them.  Each block leaves its
+// contribution alpha^k * dot_k in contrib[k]; the last block to finish (a
+// ticket, reset by it) XORs them into the enforced sum.
+__global__ void __launch_bounds__(256) k_induce_sp(const uint32_t *__restrict__ rows, uint32_t glen,
+                                                   const uint64_t *__restrict__ q, uint32_t nq, uint32_t alpha,
+                                                   uint32_t n, uint32_t b, InduceSetupArgs args,
+                                                   const uint32_t *d_rs, uint32_t nch, const uint32_t *d_alpha,
+                                                   uint32_t *__restrict__ contrib, uint32_t *__restrict__ lo,
+                                                   uint32_t *__restrict__ hi, uint32_t *sum_out, int in_smem,
+                                                   uint32_t *__restrict__ out, uint32_t *ticket, InduceStrides st) {
+    pdl_begin();
+    {
+        const uint32_t pb = blockIdx.y;  // lockstep batch: proof pb
+        rows += pb * st.rows;
+        q += pb * st.q;
+        contrib += pb * st.apow;
+        lo += pb * st.lo;
+        hi += pb * st.hi;
+        sum_out += pb * st.sum;
+        out += pb * st.out;
+        if (d_rs) d_rs += pb * st.rs;
+        if (d_alpha) d_alpha += pb * st.alpha;
+        ticket += pb;
+    }
+    // induce_main XORs its partial sums into the basis: zero it first
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (1ull << n);
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = 0;
+    extern __shared__ uint32_t sbuf[];  // Lo then Hi, when in_smem
+    __shared__ uint32_t gr[256], Ss[32], apk;
+    __shared__ bool last;
+    for (uint32_t j = threadIdx.x; j < glen; j += blockDim.x) gr[j] = d_rs ? lagrange_at(d_rs, nch, j) : args.gr[j];
+    if (d_alpha) alpha = *d_alpha;
+    __syncthreads();
+    const uint32_t k = blockIdx.x, lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {  // the setup of query k (as k_induce_setup)
+        uint32_t dot = 0;
+        for (uint32_t j = lane; j < glen; j += 32) dot ^= gf_mul(rows[(uint64_t)k * glen + j], gr[j]);
+        dot = warp_xor(dot);
+        uint32_t a2 = alpha;
+        for (uint32_t i = 0; i < lane && i < 16; ++i) a2 = gf_mul(a2, a2);
+        uint32_t pw = (lane < 16 && ((k >> lane) & 1)) ? a2 : 1u;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) pw = gf_mul(pw, __shfl_xor_sync(0xffffffffu, pw, o));
+        pw = __shfl_sync(0xffffffffu, pw, 0);
+        if (lane == 0) {
+            apk = pw;
+            contrib[k] = gf_mul(dot, pw);
+            uint32_t sx = (uint32_t)q[k];
+            if (n) Ss[0] = sx;
+            for (uint32_t i = 1; i < n; ++i) {
+                sx = gf_mul(sx, sx) ^ gf_mul(args.sks[i - 1], sx);
+                Ss[i] = sx;
+            }
+        }
+    }
+    __syncthreads();
+    // the prep of query k (as k_induce_prep)
+    const uint32_t nlo = 1u << b, nhi = 1u << (n - b);
+    uint32_t *glk = lo + ((uint64_t)k << b), *ghk = hi + ((uint64_t)k << (n - b));
+    uint32_t *lk = in_smem ? sbuf : glk, *hk = in_smem ? sbuf + nlo : ghk;
+    if (threadIdx.x == 0) {
+        lk[0] = 1;
+        hk[0] = apk;
+    }
+    __syncthreads();
+    for (uint32_t h = 0; h < b; ++h) {
+        const uint32_t sv = Ss[h];
+        for (uint32_t u = threadIdx.x; u < (1u << h); u += blockDim.x) lk[(1u << h) + u] = gf_mul(lk[u], sv);
+        __syncthreads();
+    }
+    for (uint32_t h = 0; h < n - b; ++h) {
+        const uint32_t sv = Ss[b + h];
+        for (uint32_t c = threadIdx.x; c < (1u << h); c += blockDim.x) hk[(1u << h) + c] = gf_mul(hk[c], sv);
+        __syncthreads();
+    }
+    if (in_smem) {
+        for (uint32_t u = threadIdx.x; u < nlo; u += blockDim.x) glk[u] = lk[u];
+        for (uint32_t c = threadIdx.x; c < nhi; c += blockDim.x) ghk[c] = hk[c];
+    }
+    // the enforced sum, by the last block to finish
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    uint32_t x = 0;
+    for (uint32_t j = lane; j < nq; j += 32) x ^= __ldcg(contrib + j);
+    x = warp_xor(x);
+    if (lane == 0) {
+        *sum_out = x;
+        *ticket = 0;
+    }
+}
+
+cudaError_t induce_fused(Launcher &L, const InducePlan &p, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
+                         const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
+                         uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs, const uint32_t *d_alpha,
+                         uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum, uint32_t B,
+                         const InduceStrides &st) {
+    if (!L.tickets || B > kMaxTickets || n > 32 || n == 0) {
+        cudaError_t e = induce_setup(L, d_rows, glen, gr, d_q, nq, alpha, n, sks, d_S, d_apow, d_rs, d_alpha, B, st);
+        if (e != cudaSuccess) return e;
+        return induce_basis(L, p, d_S, d_apow, n, nq, d_lo, d_hi, out, d_sum, B, st);
+    }
+    if (glen > 256 || nq == 0 || nq > 65536 || (glen & (glen - 1)) || (!gr && !d_rs) || B == 0 || B > 65535)
+        return cudaErrorInvalidValue;
+    InduceSetupArgs args{};
+    if (!d_rs)
+        for (uint32_t j = 0; j < glen; ++j) args.gr[j] = gr[j];
+    for (uint32_t i = 0; i + 1 < n && i < 32; ++i) args.sks[i] = sks[i];
+    const double vec = (double)nq * ((1ull << p.b) + (1ull << (n - p.b)));
+    L.note(4.0 * B * (vec + nq * (glen + 2)), B * (vec + nq * (glen + 2.0 * n + 20)));
+    const size_t words = (1ull << p.b) + (1ull << (n - p.b));
+    const int in_smem = words <= 10240;  // with the static arrays, under the 48 KB that needs no opt-in
+    LGK_LAUNCH(L, "induce_sp", launch_k(k_induce_sp, dim3(nq, B), 256, in_smem ? 4 * words : 0, L.stream, d_rows, glen,
+                                        d_q, nq, alpha, n, p.b, args, d_rs, ilog2u(glen), d_alpha, d_apow, d_lo, d_hi,
+                                        d_sum, in_smem, out, L.tickets, st));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_induce_main(L, p, n, nq, d_lo, d_hi, out, B, st);
 }
 
 // ====================================================== opening check

@@ -249,6 +249,14 @@ cudaError_t induce_setup(Launcher &L, const uint32_t *d_rows, uint32_t glen, con
                          uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs = nullptr,
                          const uint32_t *d_alpha = nullptr, uint32_t B = 1,
                          const InduceStrides &st = InduceStrides{});
+// induce_setup and induce_basis with the setup and the prep in one launch
+// (its last block sums the enforced sum; needs the Launcher's tickets, and
+// otherwise runs the two calls).  d_S is used only by that fallback.
+cudaError_t induce_fused(Launcher &L, const InducePlan &p, const uint32_t *d_rows, uint32_t glen, const uint32_t *gr,
+                         const uint64_t *d_q, uint32_t nq, uint32_t alpha, uint32_t n, const uint32_t *sks,
+                         uint32_t *d_S, uint32_t *d_apow, const uint32_t *d_rs, const uint32_t *d_alpha,
+                         uint32_t *d_lo, uint32_t *d_hi, uint32_t *out, uint32_t *d_sum, uint32_t B = 1,
+                         const InduceStrides &st = InduceStrides{});
 
 cudaError_t splitmix(Launcher &L, uint64_t seed, uint32_t *out, uint64_t n);
 
