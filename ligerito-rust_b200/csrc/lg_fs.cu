@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a,
     __shared__ uint32_t hrank[kHash];
     __shared__ uint32_t lo32[kQBlock];
     __shared__ uint32_t scratch[kQBlock / 32];
-    __shared__ uint32_t wcnt[64][kQBlock / 32];
+    __shared__ uint32_t wcnt[64][kQBlock / 32], wmask[64][kQBlock / 32];
     __shared__ uint32_t take_sh, batch_sh;
     __shared__ uint32_t kw[kMaxChain][64];
     const uint32_t tid = threadIdx.x;
@@ -255,10 +255,16 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a,
         // Per-warp counts of every layer, then one scan gives each warp its
         // start in each layer (layers in order, threads in query order):
         // two barriers instead of two per layer.
-        uint64_t x;
+        // (each layer's emit bit and warp mask are kept for the write pass)
+        uint64_t x, emask = 0;
         for (uint32_t d = 0; d < nl; ++d) {
-            const uint32_t m = __ballot_sync(0xffffffffu, emits(d, x));
-            if (lane == 0) wcnt[d][warp] = __popc(m);
+            const bool e = emits(d, x);
+            emask |= (uint64_t)e << d;
+            const uint32_t m = __ballot_sync(0xffffffffu, e);
+            if (lane == 0) {
+                wcnt[d][warp] = __popc(m);
+                wmask[d][warp] = m;
+            }
         }
         __syncthreads();
         if (warp == 0) {
@@ -295,10 +301,10 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a,
         __syncthreads();
         uint64_t layer_off = 0, width = a.n;
         for (uint32_t d = 0; d < nl; ++d) {
-            const bool e = emits(d, x);
-            const uint32_t m = __ballot_sync(0xffffffffu, e);
+            const bool e = (emask >> d) & 1;
+            const uint32_t m = wmask[d][warp];
             const uint32_t pos = wcnt[d][warp] + __popc(m & ((1u << lane) - 1));
-            if (e && pos < a.nodes_cap) a.nodes[pos] = layer_off + (x ^ 1);
+            if (e && pos < a.nodes_cap) a.nodes[pos] = layer_off + ((qi >> d) ^ 1);
             layer_off += width;
             width >>= 1;
         }

@@ -21,6 +21,18 @@ __constant__ uint32_t kK256[64] = {
     0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
 
 __device__ __forceinline__ uint32_t rr(uint32_t x, int r) { return __funnelshift_r(x, x, r); }
+
+// x + y on the multiply-add pipe (y * 1 + x, the 1 read from constant
+// memory so the compiler keeps the multiply-add).  The transcript runs on
+// one thread, whose rounds are bound by the logic pipe's issue rate (a
+// warp instruction occupies its 16 lanes for two cycles): the rotations and
+// logic stay there, the additions move to the otherwise idle pipe.
+__constant__ uint32_t kOne = 1u;
+__device__ __forceinline__ uint32_t addm(uint32_t x, uint32_t y) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(y), "r"(kOne), "r"(x));
+    return r;
+}
 __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 
 // FIPS 180-4 compression of one block of 16 big-endian words (registers).
@@ -39,18 +51,18 @@ __device__ __forceinline__ void sha_compress(uint32_t st[8], const uint32_t (&bl
     for (int t0 = 0; t0 < 64; t0 += 8) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const uint32_t hk = h + kK256[t0 + i] + w[i];  // independent of e: off the serial path
-            const uint32_t t1 = hk + (rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)) + ((e & f) ^ (~e & g));
-            const uint32_t t2 = (rr(a, 2) ^ rr(a, 13) ^ rr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
-            h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+            const uint32_t hk = addm(addm(h, kK256[t0 + i]), w[i]);  // independent of e: off the serial path
+            const uint32_t t1 = addm(addm(hk, rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)), (e & f) ^ (~e & g));
+            const uint32_t t2 = addm(rr(a, 2) ^ rr(a, 13) ^ rr(a, 22), (a & b) ^ (a & c) ^ (b & c));
+            h = g; g = f; f = e; e = addm(d, t1); d = c; c = b; b = a; a = addm(t1, t2);
         }
         if (t0 < 48) {
             uint32_t nw[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
                 const uint32_t x = w[i + 1], y = i >= 2 ? nw[i - 2] : w[i + 14];
-                nw[i] = (rr(x, 7) ^ rr(x, 18) ^ (x >> 3)) + w[i] + (i >= 7 ? nw[0] : w[i + 9]) +
-                        (rr(y, 17) ^ rr(y, 19) ^ (y >> 10));
+                nw[i] = addm(addm(addm(rr(x, 7) ^ rr(x, 18) ^ (x >> 3), w[i]), i >= 7 ? nw[0] : w[i + 9]),
+                             rr(y, 17) ^ rr(y, 19) ^ (y >> 10));
             }
 #pragma unroll
             for (int i = 0; i < 8; ++i) { w[i] = w[i + 8]; w[i + 8] = nw[i]; }
@@ -59,7 +71,8 @@ __device__ __forceinline__ void sha_compress(uint32_t st[8], const uint32_t (&bl
             for (int i = 0; i < 8; ++i) w[i] = w[i + 8];
         }
     }
-    st[0] += a; st[1] += b; st[2] += c; st[3] += d; st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+    st[0] = addm(st[0], a); st[1] = addm(st[1], b); st[2] = addm(st[2], c); st[3] = addm(st[3], d);
+    st[4] = addm(st[4], e); st[5] = addm(st[5], f); st[6] = addm(st[6], g); st[7] = addm(st[7], h);
 }
 
 // The 64 rounds of a compression whose K[t] + W[t] are already in kw (the
@@ -70,13 +83,14 @@ __device__ __forceinline__ void sha_rounds_kw(uint32_t st[8], const uint32_t *kw
     for (int t0 = 0; t0 < 64; t0 += 16) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-            const uint32_t hk = h + kw[t0 + i];
-            const uint32_t t1 = hk + (rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)) + ((e & f) ^ (~e & g));
-            const uint32_t t2 = (rr(a, 2) ^ rr(a, 13) ^ rr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
-            h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+            const uint32_t hk = addm(h, kw[t0 + i]);
+            const uint32_t t1 = addm(addm(hk, rr(e, 6) ^ rr(e, 11) ^ rr(e, 25)), (e & f) ^ (~e & g));
+            const uint32_t t2 = addm(rr(a, 2) ^ rr(a, 13) ^ rr(a, 22), (a & b) ^ (a & c) ^ (b & c));
+            h = g; g = f; f = e; e = addm(d, t1); d = c; c = b; b = a; a = addm(t1, t2);
         }
     }
-    st[0] += a; st[1] += b; st[2] += c; st[3] += d; st[4] += e; st[5] += f; st[6] += g; st[7] += h;
+    st[0] = addm(st[0], a); st[1] = addm(st[1], b); st[2] = addm(st[2], c); st[3] = addm(st[3], d);
+    st[4] = addm(st[4], e); st[5] = addm(st[5], f); st[6] = addm(st[6], g); st[7] = addm(st[7], h);
 }
 
 // K[t] + W[t] (t < 64) of a block of 16 big-endian words.
