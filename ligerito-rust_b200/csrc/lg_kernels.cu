@@ -1073,31 +1073,31 @@ __global__ void __launch_bounds__(256) k_fold_eq(const uint32_t *__restrict__ in
             if (g + gstride < groups) load_all(g + gstride);
             out[g] = acc;
         }
-        return;
-    }
-    for (; g < groups; g += gstride) {
-        const uint32_t *src = in + g * V;
-        uint32_t acc[V];
+    } else {
+        for (; g < groups; g += gstride) {
+            const uint32_t *src = in + g * V;
+            uint32_t acc[V];
 #pragma unroll
-        for (int x = 0; x < V; ++x) acc[x] = 0;
+            for (int x = 0; x < V; ++x) acc[x] = 0;
 #pragma unroll
-        for (int jh = 0; jh < NH; ++jh) {
-            uint32_t v[NL][V];
+            for (int jh = 0; jh < NH; ++jh) {
+                uint32_t v[NL][V];
 #pragma unroll
-            for (int jl = 0; jl < NL; ++jl) {
-                const uint32_t *p = src + (uint64_t)(jh * NL + jl) * M;
-                const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
-                v[jl][0] = t.x; v[jl][1] = t.y; v[jl][2] = t.z; v[jl][3] = t.w;
+                for (int jl = 0; jl < NL; ++jl) {
+                    const uint32_t *p = src + (uint64_t)(jh * NL + jl) * M;
+                    const uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+                    v[jl][0] = t.x; v[jl][1] = t.y; v[jl][2] = t.z; v[jl][3] = t.w;
+                }
+#pragma unroll
+                for (int x = 0; x < V; ++x) {
+                    uint32_t part = 0;
+#pragma unroll
+                    for (int jl = 0; jl < NL; ++jl) part ^= tab_mul_sa(t8, 512u * jl, 0, v[jl][x]);
+                    acc[x] ^= KH ? tab_mul_sa(t8, 512u * (NL + jh), 0, part) : part;
+                }
             }
-#pragma unroll
-            for (int x = 0; x < V; ++x) {
-                uint32_t part = 0;
-#pragma unroll
-                for (int jl = 0; jl < NL; ++jl) part ^= tab_mul_sa(t8, 512u * jl, 0, v[jl][x]);
-                acc[x] ^= KH ? tab_mul_sa(t8, 512u * (NL + jh), 0, part) : part;
-            }
+            *reinterpret_cast<uint4 *>(out + g * 4) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
         }
-        *reinterpret_cast<uint4 *>(out + g * 4) = make_uint4(acc[0], acc[1], acc[2], acc[3]);
     }
 }
 
