@@ -148,6 +148,8 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a,
     __shared__ uint32_t lo32[kQBlock];
     __shared__ uint32_t scratch[kQBlock / 32];
     __shared__ uint32_t wcnt[64][kQBlock / 32], wmask[64][kQBlock / 32];
+    __shared__ uint64_t sq[kQBlock];     // a batch's squeezes, by index
+    __shared__ uint32_t order[kQBlock];  // squeeze index of each thread
     __shared__ uint32_t take_sh, batch_sh;
     __shared__ uint32_t kw[kMaxChain][64];
     const uint32_t tid = threadIdx.x;
@@ -169,9 +171,25 @@ __global__ void __launch_bounds__(kQBlock) k_fs_queries(FsState *g, FsQueries a,
         const uint64_t want = need + margin + a.nsq;
         batch = want < kQBlock ? (uint32_t)want : kQBlock;
         fs_chain_block(S, B, batch, kw);
+        // A squeeze whose final data fills 14 or 15 words of its last block
+        // needs a second compression for the padding; those squeezes go to
+        // the first threads, so that only their warps run two compressions
+        // (each warp of consecutive squeezes would otherwise hold some).
+        {
+            const bool two = tid < batch && ((S.nw + tid + 1) & 15) >= 14;
+            uint32_t total2;
+            const uint32_t r2 = block_rank(two, scratch, &total2);
+            if (tid < batch) order[two ? r2 : total2 + (tid - r2)] = tid;
+        }
+        __syncthreads();
+        if (tid < batch) {
+            const uint32_t i = order[tid];
+            sq[i] = fs_squeeze_at(S, B, i);
+        }
+        __syncthreads();
         uint64_t qv = 0;
         if (tid < batch) {
-            const uint64_t lo = fs_squeeze_at(S, B, tid);
+            const uint64_t lo = sq[tid];
             lo32[tid] = (uint32_t)lo;
             qv = lo & mask;
         }
