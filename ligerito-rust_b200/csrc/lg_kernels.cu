@@ -817,26 +817,40 @@ __global__ void __launch_bounds__(128) k_merkle_thread3(uint32_t *__restrict__ t
     if (8 * t >= n_in) return;
     const uint64_t off1 = in_off + n_in, off2 = off1 + n_in / 2, off3 = off2 + n_in / 4;
     const uint32_t *src = tree + 8 * (in_off + 8 * t);
-    uint32_t q[8], l[8], r[8], n01[8], n23[8];
+    // The 7 nodes in post order, one compression per iteration (a single
+    // copy of it in the code: seven inlined copies stalled on instruction
+    // fetch): i = 0, 1 hash leaf pairs 0, 1 into layer-1 nodes A0, A1; i = 2
+    // hashes (A0, A1) into B0; i = 3, 4 leaf pairs 2, 3 into A2, A3; i = 5
+    // (A2, A3) into B1; i = 6 (B0, B1) into the layer-3 node.
+    uint32_t l[8], r[8], h[8], a[8], b[8];
+    load_node(src, l);
+    load_node(src + 8, r);
+#pragma unroll 1
+    for (uint32_t i = 0; i < 7; ++i) {
+        hash_pair(l, r, h, one);
+        const uint64_t at = (i == 6)                ? off3 + t
+                            : (i == 2 || i == 5)    ? off2 + 2 * t + (i == 5)
+                                                    : off1 + 4 * t + (i < 2 ? i : i - 1);
+        store_node(tree + 8 * at, h);
+        if (i == 0 || i == 2 || i == 3) {
+            // the next compression hashes leaf pair 1 (after i = 0), 2 or 3
+            if (i != 2) {
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        const uint32_t *s4 = src + 32 * half;  // children 4*half .. 4*half+3
-        load_node(s4, l);
-        load_node(s4 + 8, r);
-        hash_pair(l, r, n01, one);
-        store_node(tree + 8 * (off1 + 4 * t + 2 * half), n01);
-        load_node(s4 + 16, l);
-        load_node(s4 + 24, r);
-        hash_pair(l, r, n23, one);
-        store_node(tree + 8 * (off1 + 4 * t + 2 * half + 1), n23);
-        if (half == 0) {
-            hash_pair(n01, n23, q, one);
-            store_node(tree + 8 * (off2 + 2 * t), q);
+                for (int w = 0; w < 8; ++w) a[w] = h[w];
+            } else {
+#pragma unroll
+                for (int w = 0; w < 8; ++w) b[w] = h[w];
+            }
+            const uint32_t *s = src + 16 * (i == 0 ? 1 : i);
+            load_node(s, l);
+            load_node(s + 8, r);
         } else {
-            hash_pair(n01, n23, l, one);
-            store_node(tree + 8 * (off2 + 2 * t + 1), l);
-            hash_pair(q, l, r, one);
-            store_node(tree + 8 * (off3 + t), r);
+            // i = 1, 4: (a, h) are the two layer-1 children; i = 5: (b, h)
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                l[w] = i == 5 ? b[w] : a[w];
+                r[w] = h[w];
+            }
         }
     }
 }
